@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""POGM iterations/s of the MSLR hot path on B200.
+
+Workload (the metric's configuration): N = (90, 90, 60) complex64, 18 coils,
+Nt = 300, two scales — the global 90x90x60 patch and 10^3 patches with
+stride 10 — on seeded synthetic data of those shapes (rank-8 temporal basis,
+1/6 sampling with a 12^3 centre, normalised as run_recon does).  One step is
+one POGM iteration: the SENSE normal operator, the fused u/z update with the
+FP64 restart sums, and patch SVST over both scales.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU) runs independent replicas (weak
+scaling); the value is the sum of iterations/s over ranks with the time
+taken as the max over ranks.  ``--impl reference`` times the CPU port of the
+reference algorithm (Julia is not available) on rank 0's host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "metric"
+
+
+def load_problem(name: str, seed_offset: int = 0):
+    """Seeded synthetic problem of the named workload (the generator module is
+    loaded by path so that the CPU-only reference arm needs no GPU library)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mslr_synth_bench",
+                                                  os.path.join(ROOT, "mslr-recon_b200", "synth.py"))
+    S = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(S)
+    import dataclasses
+    cfg = dataclasses.replace(S.CONFIGS[name], seed=S.CONFIGS[name].seed + seed_offset)
+    fft = "scipy"
+    try:
+        import torch
+        if torch.cuda.is_available():
+            fft = "torch"
+    except Exception:
+        pass
+    t0 = time.perf_counter()
+    pb = S.make_problem(cfg, fft=fft)
+    log(f"generated {name} problem in {time.perf_counter() - t0:.1f}s ({fft} FFT)")
+    return pb
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--form", default="tuned", choices=["tuned", "plain"])
+    p.add_argument("--workload", default=WORKLOAD)
+    p.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison")
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--phases", action="store_true", help="print per-phase timings to stderr")
+    return p.parse_args()
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU port (oracle restatement in FP32, all host threads) — bounded sample
+# ---------------------------------------------------------------------------
+def cpu_sample_iteration(pb, frac_frames: float, frac_patches: float, frac_rows: float, seed=0):
+    """Time a bounded sample of one POGM iteration of the CPU port and scale
+    it to a full iteration.  Returns (seconds_per_iteration, description)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import mslr_oracle as O
+    ncores = os.cpu_count() or 1
+    smaps = pb["smaps"]
+    idx = pb["idx"]
+    y = pb["y"]
+    Nt = y.shape[0]
+    Nx, Ny, Nz = pb["N"]
+    rng = np.random.default_rng(seed)
+    x = pb["x_true"]
+    # (a) data-consistency gradient on a subset of frames
+    nf = max(1, int(round(frac_frames * Nt)))
+    t0 = time.perf_counter()
+    for t in range(nf):
+        r = O.sense_forward_frame(x[t], smaps, idx[t], workers=ncores) - y[t]
+        O.sense_adjoint_frame(r.astype(np.complex64), smaps, idx[t], workers=ncores)
+    ta = (time.perf_counter() - t0) * Nt / nf
+    # (b) local-scale SVST on a subset of patches (gesdd, thread pool)
+    ps = pb["patch_sizes"][1]
+    g = O.patch_geometry(pb["N"], ps, pb["strides"][1])
+    npatch = max(1, int(round(frac_patches * g.Np)))
+    mats = []
+    for ip in rng.choice(g.Np, npatch, replace=False):
+        sx, sy, sz = g.patch_start(int(ip))
+        blk = x[:, sz:sz + ps[2], sy:sy + ps[1], sx:sx + ps[0]].reshape(Nt, -1).T.copy()
+        mats.append(blk)
+    lam = O.ong_lustig_lambdas(pb["N"], Nt, pb["patch_sizes"])
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(ncores) as ex:
+        list(ex.map(lambda m: O.svst(m, lam[1]), mats))
+    tb = (time.perf_counter() - t0) * g.Np / npatch
+    # (c) global patch: thin SVD cost is linear in rows — time a row subset
+    nvox = Nx * Ny * Nz
+    nrow = max(Nt, int(round(frac_rows * nvox)))
+    G = x.reshape(Nt, nvox)[:, :nrow].T.copy()
+    t0 = time.perf_counter()
+    O.svst(G, lam[0])
+    tc = (time.perf_counter() - t0) * nvox / nrow
+    # (d) POGM elementwise on the same row subset, two scales
+    xs = np.stack([x.reshape(Nt, nvox)[:, :nrow]] * 2)
+    us = xs.copy()
+    gg = x.reshape(Nt, nvox)[:, :nrow]
+    t0 = time.perf_counter()
+    un = xs - np.float32(0.5) * gg[None]
+    zn = un + np.float32(0.3) * (un - us) + np.float32(0.6) * (un - xs)
+    float(np.sum(np.real(-gg[None] * (un - us)), dtype=np.float64))
+    td = (time.perf_counter() - t0) * nvox / nrow
+    del zn
+    total = ta + tb + tc + td
+    desc = (f"FP32 numpy/scipy port, {ncores} threads: normal op on {nf}/{Nt} frames, gesdd SVST on "
+            f"{npatch}/{g.Np} 10^3 patches, global-patch SVD on {nrow}/{nvox} rows, POGM update on "
+            f"the same rows; each scaled to one full iteration")
+    return total, desc, ncores
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pb = load_problem(args.workload)
+    secs = []
+    desc = ""
+    cores = 1
+    for i in range(args.warmup + args.steps):
+        s, desc, cores = cpu_sample_iteration(pb, 2 / 300, 6 / 486, 1 / 60, seed=i)
+        if i >= args.warmup:
+            secs.append(s)
+    v = 1.0 / (sum(secs) / len(secs))
+    line = {"metric": "POGM iter/s (90x90x60, 18 coils, Nt=300, 2 scales)", "value": v,
+            "unit": "iter/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": "90x90x60, 18 coils, Nt=300, scales [90,90,60]+[10,10,10] stride=size"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "iter/s", "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def time_steps(torch, ctx, X, steps, stream):
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        ctx.pogm_step(X, stream=stream)
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1) / 1000.0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import mslr_recon_b200 as M
+    pb = load_problem(args.workload, seed_offset=rank)
+    Nt, Nc, K = pb["y"].shape
+    Nx, Ny, Nz = pb["N"]
+    nvox = Nx * Ny * Nz
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    # host (pinned) inputs for the end-to-end leg
+    h_smaps = torch.from_numpy(pb["smaps"]).pin_memory()
+    h_y = torch.from_numpy(pb["y"]).pin_memory()
+    h_idx = torch.from_numpy(pb["idx"]).pin_memory()
+    L = float(len(pb["patch_sizes"]))   # σ1 = 1 (σ1A_PRECOMPUTED = 1.0 as the experiment files)
+
+    def device_run(form, steps, warmup):
+        ctx = M.MSLRContext(pb["N"], Nc, Nt, K, pb["patch_sizes"], pb["strides"], form=form)
+        ctx.bind(h_smaps.to(dev), h_y.to(dev), h_idx.to(dev))
+        X = ctx.init_x0()
+        ctx.pogm_begin(X, warmup + steps, L)
+        for _ in range(warmup):
+            ctx.pogm_step(X)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        n0 = ctx.launch_count()
+        clocks = Clocks(local)
+        clocks.start()
+        secs = time_steps(torch, ctx, X, steps, stream)
+        ck = clocks.stop()
+        launches = ctx.launch_count() - n0
+        torch.cuda.synchronize()
+        if world > 1:
+            t = torch.tensor([secs], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            secs = float(t.item())
+        return ctx, X, secs, ck, launches
+
+    ctx, X, secs, clocks, launches = device_run(args.form, args.steps, args.warmup)
+    value = world * args.steps / secs
+
+    # per-phase timing (same stream, CUDA events) for the roofline
+    def ev_time(fn, reps=3):
+        fn()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1000.0 / reps
+
+    g = torch.empty((Nt, Nz, Ny, Nx), dtype=torch.complex64, device=dev)
+    t_normal = ev_time(lambda: ctx.normal(X, out=g))
+    tmp = torch.empty_like(g)
+    t_svst = [ev_time(lambda k=k: ctx.patch_svst(k, 0.9 * ctx.lambdas[k], X[k], out=tmp))
+              for k in range(ctx.Ns)]
+    phases = {"normal_op_ms": t_normal * 1e3, "svst_ms": [t * 1e3 for t in t_svst]}
+    if args.phases:
+        log("phases", json.dumps(phases))
+    # roofline of the dominant phase (HBM-bound: algorithmic bytes / time)
+    from mslr_recon_b200 import roofline as RL
+    peaks = RL.peaks()
+    Ns = len(pb["patch_sizes"])
+    dom = "normal_op" if t_normal >= max(t_svst) else f"svst_scale{int(np.argmax(t_svst))}"
+    if dom == "normal_op":
+        byts = RL.normal_op_bytes(nvox, Nt, Nc, Ns)
+        tdom = t_normal
+    else:
+        k = int(np.argmax(t_svst))
+        byts = RL.svst_bytes(nvox, Nt)
+        tdom = t_svst[k]
+    achieved = byts / tdom / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
+            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+            "algorithmic_bytes": byts, "peak_source": peaks["source"]}
+
+    plain_ips = None
+    if not args.no_plain and args.form == "tuned":
+        del ctx
+        torch.cuda.empty_cache()
+        pctx, pX, psecs, _, _ = device_run("plain", max(2, args.steps // 2), 1)
+        plain_ips = world * max(2, args.steps // 2) / psecs
+        del pctx, pX
+    else:
+        del ctx
+    torch.cuda.empty_cache()
+
+    # end-to-end through the public API with host buffers (H2D + bind + POGM + D2H)
+    e2e = None
+    if not args.no_e2e:
+        niter = args.steps
+        h_out = torch.empty((Ns, Nt, Nz, Ny, Nx), dtype=torch.complex64).pin_memory()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d_s, d_y, d_i = (h_smaps.to(dev, non_blocking=True), h_y.to(dev, non_blocking=True),
+                         h_idx.to(dev, non_blocking=True))
+        ectx = M.MSLRContext(pb["N"], Nc, Nt, K, pb["patch_sizes"], pb["strides"], form=args.form)
+        ectx.bind(d_s, d_y, d_i)
+        EX = ectx.init_x0()
+        ectx.pogm_run(EX, niter, L)
+        h_out.copy_(EX, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        esecs = e0.elapsed_time(e1) / 1000.0
+        if world > 1:
+            t = torch.tensor([esecs], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            esecs = float(t.item())
+        h2d = h_smaps.numel() * 8 + h_y.numel() * 8 + h_idx.numel() * 4
+        d2h = h_out.numel() * 8
+        e2e = {"value": world * niter / esecs, "unit": "iter/s",
+               "h2d_bytes_per_step": h2d / niter, "d2h_bytes_per_step": d2h / niter,
+               "note": f"one run_recon-style call of {niter} iterations per measurement; "
+                       "inputs copied once per call, bytes shown per iteration"}
+        ectx.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        s, desc, cores = cpu_sample_iteration(pb, 4 / 300, 12 / 486, 1 / 30)
+        cpu = {"value": 1.0 / s, "unit": "iter/s", "cores": cores, "kind": "port", "sample": desc}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {"metric": "POGM iter/s (90x90x60, 18 coils, Nt=300, 2 scales)", "value": value,
+                "unit": "iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+                "config": {"workload": "90x90x60, 18 coils, Nt=300, scales [90,90,60]+[10,10,10] stride=size",
+                           "form": args.form, "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (X is 2.3 GB)",
+                           "plain_form_iter_s": plain_ips,
+                           "tuned_over_plain": (value / world / plain_ips * world) if plain_ips else None,
+                           "phases": phases},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

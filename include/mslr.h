@@ -1,0 +1,173 @@
+/*
+ * mslr.h — C ABI of the B200 (sm_100a) MSLR hot-path library, libmslr.so.
+ *
+ * Replaces, for one GPU, the per-iteration path of rextlfung/mslr-recon:
+ *   - the SENSE operator            src/sense_gpu.jl:56-108   (Asense_gpu fwd/adj)
+ *   - the data-consistency gradient scripts/reconstruct.jl:180-183 (dc_cost_grad)
+ *   - patch SVST with extract/recombine
+ *                                   src/recon.jl:53-126, :183-269,
+ *                                   src/sense_gpu.jl:122-223 (patchSVST_gpu)
+ *   - POGM with gradient restart    src/mirt_mod.jl:26-29, :74-188 (pogm_mod)
+ *   - power iteration               src/mirt_mod.jl:215-238 (poweriter_mod)
+ *   - run_recon's closures and X0   scripts/reconstruct.jl:159-214
+ *
+ * Conventions (those of the reference's Julia arrays):
+ *   - complex data are interleaved float pairs (ComplexF32), column-major:
+ *       image        (Nx, Ny, Nz, Nt)          X (Nx, Ny, Nz, Nt, Ns)
+ *       coil maps    (Nx, Ny, Nz, Nc)          k-space y (K, Nc, Nt)
+ *       patch stack  (p, Nt, Np)
+ *     so x is the fastest index everywhere;
+ *   - sample indices idx (K, Nt) are int32 linear indices into the centred
+ *     (Nx, Ny, Nz) k-space grid, ascending per frame — the reference's
+ *     findall(vec(samp)) — 1-based when index_base == 1, 0-based when 0;
+ *   - every device pointer is BORROWED: the library never frees caller
+ *     memory; all workspaces are owned by the context and allocated in
+ *     mslr_create / mslr_bind, never inside the per-iteration calls;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default);
+ *   - every call returns an int status (MSLR_OK == 0) and never aborts;
+ *     mslr_last_error() returns a message for the last failure on a context
+ *     (or, with ctx == NULL, for the calling thread's last context-free call);
+ *   - one context must not be used from two host threads at once.
+ */
+#ifndef MSLR_H
+#define MSLR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MSLR_ABI_VERSION 1
+
+#define MSLR_OK 0
+#define MSLR_ERR_ARG 1           /* bad shape, pointer or value (ArgumentError / @assert) */
+#define MSLR_ERR_CUDA 2          /* a CUDA runtime call failed */
+#define MSLR_ERR_STATE 3         /* call out of order (e.g. before mslr_bind) */
+#define MSLR_ERR_UNSUPPORTED 4   /* shape outside what the kernels support */
+#define MSLR_ERR_NONFINITE 5     /* NaN/Inf met in a reduction */
+#define MSLR_ERR_NOMEM 6         /* device allocation failed */
+
+/* Computation forms (mslr_create `form`). */
+#define MSLR_FORM_PLAIN 0        /* FP32 SIMT Gram/rebuild, one launch sequence per scale, no graph */
+#define MSLR_FORM_TUNED 1        /* split-precision tensor-core Gram/rebuild, graph-captured iteration */
+
+typedef struct mslr_ctx mslr_ctx;
+
+/* Library ABI version (MSLR_ABI_VERSION). */
+int mslr_abi_version(void);
+
+/* Last error message for `ctx` (ctx == NULL: the calling thread's last
+ * context-free error).  The string stays valid until the next failing call. */
+const char* mslr_last_error(const mslr_ctx* ctx);
+
+/* ------------------------------------------------------------------------
+ * Patch geometry (host only) — src/recon.jl:54-72.
+ * For one scale: clamps ps to N, nsteps[d] = cld(N[d]-ps[d], ss[d]),
+ * Np = prod(nsteps+1).  `starts` (optional, may be NULL) receives the
+ * 0-based patch starts of each dimension concatenated:
+ * (nsteps[0]+1) x-starts, then y-starts, then z-starts.
+ * ------------------------------------------------------------------------ */
+int mslr_patch_geometry(const int32_t N[3], const int32_t patch[3], const int32_t stride[3],
+                        int32_t ps_out[3], int32_t nsteps_out[3], int64_t* Np_out,
+                        int32_t* starts);
+
+/* img2patches (src/recon.jl:53-78; src/sense_gpu.jl:168-192):
+ * img (Nx,Ny,Nz,Nt) -> P (p, Nt, Np), device pointers. */
+int mslr_img2patches(const int32_t N[3], int32_t Nt, const int32_t patch[3],
+                     const int32_t stride[3], const void* img, void* P, void* stream);
+
+/* patches2img (src/recon.jl:96-126; src/sense_gpu.jl:194-223):
+ * P (p, Nt, Np) -> img (Nx,Ny,Nz,Nt): patch sums in ascending ip divided by
+ * max(coverage count, 1). */
+int mslr_patches2img(const int32_t N[3], int32_t Nt, const int32_t patch[3],
+                     const int32_t stride[3], const void* P, void* img, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Batched SVST (src/recon.jl:183-211 SVST; src/sense_gpu.jl:122-128 SVST_gpu)
+ * on `batch` independent m x n column-major complex matrices stored back to
+ * back: out_b = U diag(max(S - beta_b, 0)) V^H, zero when ||A_b|| == 0.
+ * `betas` is a host array of `batch` thresholds.  The caller provides device
+ * scratch of at least mslr_svst_batch_workspace() bytes.  in may equal out.
+ * ------------------------------------------------------------------------ */
+int mslr_svst_batch_workspace(int32_t m, int32_t n, int32_t batch, size_t* bytes);
+int mslr_svst_batch(int32_t m, int32_t n, int32_t batch, const double* betas,
+                    const void* in, void* out, void* workspace, size_t workspace_bytes,
+                    int32_t form, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Reconstruction context — the state run_recon builds
+ * (scripts/reconstruct.jl:133-214) for Ns scales of patch sizes/strides.
+ * patch/stride: 3*n_scales int32 (x,y,z per scale).  K = samples per frame
+ * (uniform across frames, scripts/reconstruct.jl:116-118).
+ * ------------------------------------------------------------------------ */
+int mslr_create(const int32_t N[3], int32_t Nc, int32_t Nt, int64_t K, int32_t n_scales,
+                const int32_t* patch, const int32_t* stride, int32_t form, mslr_ctx** out);
+int mslr_destroy(mslr_ctx* ctx);
+
+/* Device bytes the context holds (after create / bind). */
+int mslr_workspace_bytes(const mslr_ctx* ctx, size_t* bytes);
+
+/* Bind the acquisition: coil maps smaps (Nx,Ny,Nz,Nc), k-space y (K,Nc,Nt),
+ * indices idx (K,Nt).  The library keeps its own device copies of what it
+ * needs (modulated maps, per-frame sampling bitmasks, indices, A'y), so the
+ * caller may free its buffers afterwards.  Validates that indices are in
+ * range and strictly ascending per frame (MSLR_ERR_ARG otherwise). */
+int mslr_bind(mslr_ctx* ctx, const void* smaps, const void* y, const int32_t* idx,
+              int32_t index_base, void* stream);
+
+/* Asense forward over all frames (src/sense_gpu.jl:71-81 per frame,
+ * block_diag at scripts/reconstruct.jl:142): x (Nx,Ny,Nz,Nt) -> y (K,Nc,Nt). */
+int mslr_sense_forward(mslr_ctx* ctx, const void* x, void* y, void* stream);
+
+/* Exact unitary adjoint (src/sense_gpu.jl:84-101 with scale*bfft):
+ * y (K,Nc,Nt) -> x (Nx,Ny,Nz,Nt). */
+int mslr_sense_adjoint(mslr_ctx* ctx, const void* y, void* x, void* stream);
+
+/* dc_cost_grad before the repeat (scripts/reconstruct.jl:180-183):
+ * g = A'(A * sum_k X[..,k] - y) for X (Nx,Ny,Nz,Nt,ns_in); with
+ * subtract_data == 0, g = A'A * sum_k X[..,k]. */
+int mslr_normal_op(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g,
+                   int32_t subtract_data, void* stream);
+
+/* patchSVST for scale `scale` (0-based) with global threshold beta
+ * (src/recon.jl:251-256; src/sense_gpu.jl:138-145): img_in (Nx,Ny,Nz,Nt)
+ * -> img_out.  img_in may equal img_out. */
+int mslr_patch_svst(mslr_ctx* ctx, int32_t scale, double beta, const void* img_in,
+                    void* img_out, void* stream);
+
+/* X0 of scripts/reconstruct.jl:209-214: X[..,1] = A'y, other scales 0. */
+int mslr_init_x0(mslr_ctx* ctx, void* X, void* stream);
+
+/* pogm_mod (src/mirt_mod.jl:74-188) with mom=:pogm, restart=:gr and
+ * run_recon's closures (scripts/reconstruct.jl:180-202), starting from and
+ * overwriting X (Nx,Ny,Nz,Nt,Ns).  L is the Lipschitz constant
+ * (Ns*sigma1^2).  restarts_host (optional, length niter+1) receives the
+ * per-iteration restart flags (entry 0 is false, as the logger's out[1]).
+ * The reference's in-place g_prox makes xnew alias znew; this recurrence is
+ * reproduced exactly. */
+int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restart_cutoff,
+                  double bsig, uint8_t* restarts_host, void* stream);
+
+/* Stepwise POGM: mslr_pogm_begin sets up the state for `niter` iterations
+ * from X; each mslr_pogm_step runs exactly one iteration (X holds x_i
+ * after it returns, stream-ordered). */
+int mslr_pogm_begin(mslr_ctx* ctx, void* X, int32_t niter, double L, double restart_cutoff,
+                    double bsig, void* stream);
+int mslr_pogm_step(mslr_ctx* ctx, void* X, void* stream);
+/* Restart flags of the iterations run so far (host array of niter+1). */
+int mslr_pogm_restarts(mslr_ctx* ctx, uint8_t* restarts_host, void* stream);
+
+/* Number of kernels this context has launched so far (host-side count). */
+int mslr_launch_count(const mslr_ctx* ctx, uint64_t* count);
+
+/* poweriter_mod (src/mirt_mod.jl:215-238) on the block-diagonal A with
+ * x0 = ones: sigma1 = ||A x|| / ||x||, FP64 norms. */
+int mslr_power_iter(mslr_ctx* ctx, int32_t niter, double tol, double* sigma1,
+                    int32_t* iters_done, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSLR_H */

@@ -1,0 +1,197 @@
+"""Owner of one ``mslr_ctx``: the device state run_recon builds
+(scripts/reconstruct.jl:133-214) for one acquisition and patch schedule.
+
+Device arrays are ``torch`` CUDA tensors (torch is used only for device
+memory and streams).  Layouts are the reference's column-major Julia arrays
+read as C-order tensors with reversed axes: image (Nt, Nz, Ny, Nx), X
+(Ns, Nt, Nz, Ny, Nx), coil maps (Nc, Nz, Ny, Nx), k-space (Nt, Nc, K),
+indices (Nt, K).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from ._lib import FORM_PLAIN, FORM_TUNED, check, i32arr, lib
+
+FORMS = {"plain": FORM_PLAIN, "tuned": FORM_TUNED}
+
+
+def _stream_ptr(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def _dev_c64(t, shape, name):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != torch.complex64:
+        raise TypeError(f"{name} must be complex64, got {t.dtype}")
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return t
+
+
+def ong_lustig_lambdas(N, Nt, patch_sizes):
+    """scripts/reconstruct.jl:163-169 (unclamped patch sizes)."""
+    nvox = int(np.prod(N))
+    out = []
+    for ps in patch_sizes:
+        p = int(np.prod(ps))
+        out.append(math.sqrt(p) + math.sqrt(Nt) + math.sqrt(math.log(nvox * Nt / max(p, Nt))))
+    return out
+
+
+class MSLRContext:
+    """One reconstruction context.
+
+    ``N`` = (Nx, Ny, Nz); ``patch_sizes`` / ``strides`` are lists of (x, y, z)
+    triples, one per scale; ``form`` is "plain" (FP32 SIMT) or "tuned".
+    """
+
+    def __init__(self, N, Nc: int, Nt: int, K: int, patch_sizes, strides, form: str = "tuned"):
+        if len(patch_sizes) != len(strides) or not patch_sizes:
+            raise ValueError("patch_sizes and strides must be non-empty and of equal length")
+        self.N = tuple(int(v) for v in N)
+        self.Nc, self.Nt, self.K = int(Nc), int(Nt), int(K)
+        self.patch_sizes = [list(map(int, p)) for p in patch_sizes]
+        self.strides = [list(map(int, s)) for s in strides]
+        self.Ns = len(patch_sizes)
+        self.form = form
+        self.lambdas = ong_lustig_lambdas(self.N, self.Nt, self.patch_sizes)
+        torch.cuda.init()
+        h = C.c_void_p()
+        flat_p = [v for p in self.patch_sizes for v in p]
+        flat_s = [v for s in self.strides for v in s]
+        rc = lib.mslr_create(i32arr(self.N), self.Nc, self.Nt, self.K, self.Ns, i32arr(flat_p),
+                             i32arr(flat_s), FORMS[form], C.byref(h))
+        check(rc, None)
+        self._h = h
+        self.bound = False
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.mslr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _chk(self, rc):
+        check(rc, self._h)
+
+    @property
+    def img_shape(self):
+        Nx, Ny, Nz = self.N
+        return (self.Nt, Nz, Ny, Nx)
+
+    @property
+    def x_shape(self):
+        return (self.Ns,) + self.img_shape
+
+    def workspace_bytes(self) -> int:
+        b = C.c_size_t()
+        self._chk(lib.mslr_workspace_bytes(self._h, C.byref(b)))
+        return int(b.value)
+
+    # -- acquisition -----------------------------------------------------------
+    def bind(self, smaps: torch.Tensor, y: torch.Tensor, idx: torch.Tensor, index_base: int = 0,
+             stream=None):
+        """smaps (Nc,Nz,Ny,Nx) c64, y (Nt,Nc,K) c64, idx (Nt,K) int32 — all CUDA."""
+        Nx, Ny, Nz = self.N
+        _dev_c64(smaps, (self.Nc, Nz, Ny, Nx), "smaps")
+        _dev_c64(y, (self.Nt, self.Nc, self.K), "y")
+        if idx.dtype != torch.int32 or tuple(idx.shape) != (self.Nt, self.K) or not idx.is_cuda:
+            raise ValueError("idx must be a CUDA int32 tensor of shape (Nt, K)")
+        self._chk(lib.mslr_bind(self._h, smaps.data_ptr(), y.data_ptr(),
+                                C.c_void_p(idx.contiguous().data_ptr()), index_base,
+                                _stream_ptr(stream)))
+        self.bound = True
+
+    # -- operators -------------------------------------------------------------
+    def forward(self, x: torch.Tensor, stream=None) -> torch.Tensor:
+        _dev_c64(x, self.img_shape, "x")
+        y = torch.empty((self.Nt, self.Nc, self.K), dtype=torch.complex64, device=x.device)
+        self._chk(lib.mslr_sense_forward(self._h, x.data_ptr(), y.data_ptr(), _stream_ptr(stream)))
+        return y
+
+    def adjoint(self, y: torch.Tensor, stream=None) -> torch.Tensor:
+        _dev_c64(y, (self.Nt, self.Nc, self.K), "y")
+        x = torch.empty(self.img_shape, dtype=torch.complex64, device=y.device)
+        self._chk(lib.mslr_sense_adjoint(self._h, y.data_ptr(), x.data_ptr(), _stream_ptr(stream)))
+        return x
+
+    def normal(self, X: torch.Tensor, subtract_data: bool = True, out=None, stream=None):
+        """g = A'(A Σ_k X_k − y)  (or A'A Σ_k X_k); X is (ns, Nt, Nz, Ny, Nx) or 4-D."""
+        if X.dim() == 4:
+            X = X.unsqueeze(0)
+        ns = X.shape[0]
+        _dev_c64(X, (ns,) + self.img_shape, "X")
+        g = out if out is not None else torch.empty(self.img_shape, dtype=torch.complex64,
+                                                    device=X.device)
+        self._chk(lib.mslr_normal_op(self._h, X.data_ptr(), ns, g.data_ptr(),
+                                     1 if subtract_data else 0, _stream_ptr(stream)))
+        return g
+
+    def patch_svst(self, scale: int, beta: float, img: torch.Tensor, out=None, stream=None):
+        _dev_c64(img, self.img_shape, "img")
+        o = out if out is not None else torch.empty_like(img)
+        self._chk(lib.mslr_patch_svst(self._h, int(scale), float(beta), img.data_ptr(),
+                                      o.data_ptr(), _stream_ptr(stream)))
+        return o
+
+    def init_x0(self, X=None, stream=None):
+        X = X if X is not None else torch.empty(self.x_shape, dtype=torch.complex64, device="cuda")
+        _dev_c64(X, self.x_shape, "X")
+        self._chk(lib.mslr_init_x0(self._h, X.data_ptr(), _stream_ptr(stream)))
+        return X
+
+    # -- POGM --------------------------------------------------------------------
+    def pogm_run(self, X: torch.Tensor, niter: int, L: float, restart_cutoff: float = 0.0,
+                 bsig: float = 1.0, stream=None):
+        _dev_c64(X, self.x_shape, "X")
+        r = (C.c_uint8 * (niter + 1))()
+        self._chk(lib.mslr_pogm_run(self._h, X.data_ptr(), int(niter), float(L),
+                                    float(restart_cutoff), float(bsig), r, _stream_ptr(stream)))
+        return [bool(v) for v in r]
+
+    def pogm_begin(self, X, niter, L, restart_cutoff=0.0, bsig=1.0, stream=None):
+        _dev_c64(X, self.x_shape, "X")
+        self._niter = int(niter)
+        self._chk(lib.mslr_pogm_begin(self._h, X.data_ptr(), int(niter), float(L),
+                                      float(restart_cutoff), float(bsig), _stream_ptr(stream)))
+
+    def pogm_step(self, X, stream=None):
+        self._chk(lib.mslr_pogm_step(self._h, X.data_ptr(), _stream_ptr(stream)))
+
+    def pogm_restarts(self, stream=None):
+        r = (C.c_uint8 * (self._niter + 1))()
+        self._chk(lib.mslr_pogm_restarts(self._h, r, _stream_ptr(stream)))
+        return [bool(v) for v in r]
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        self._chk(lib.mslr_launch_count(self._h, C.byref(n)))
+        return int(n.value)
+
+    def power_iter(self, niter: int = 200, tol: float = 1e-6, stream=None):
+        s = C.c_double()
+        it = C.c_int32()
+        self._chk(lib.mslr_power_iter(self._h, int(niter), float(tol), C.byref(s), C.byref(it),
+                                      _stream_ptr(stream)))
+        return float(s.value), int(it.value)

@@ -1,0 +1,82 @@
+// common.cuh — shared types and helpers of libmslr (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/mslr.h"
+
+namespace mslr {
+
+typedef float2 cf;    // ComplexF32, interleaved (re, im)
+typedef double2 cd;   // ComplexF64
+
+__host__ __device__ __forceinline__ cf cmk(float r, float i) { return make_float2(r, i); }
+__host__ __device__ __forceinline__ cf cadd(cf a, cf b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ cf csub(cf a, cf b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ cf cmul(cf a, cf b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// conj(a) * b
+__host__ __device__ __forceinline__ cf cmulc(cf a, cf b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ __forceinline__ cf cconj(cf a) { return make_float2(a.x, -a.y); }
+__host__ __device__ __forceinline__ cf cscale(cf a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ float cabs2(cf a) { return a.x * a.x + a.y * a.y; }
+
+__host__ __device__ __forceinline__ cd dmk(double r, double i) { return make_double2(r, i); }
+__host__ __device__ __forceinline__ cd dadd(cd a, cd b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ cd dsub(cd a, cd b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ cd dmul(cd a, cd b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ cd dconj(cd a) { return make_double2(a.x, -a.y); }
+
+// Maximum FFT axis length handled by the shared-memory FFT.
+constexpr int kMaxFftLen = 1024;
+constexpr int kMaxPasses = 12;
+
+// Mixed-radix plan of one axis (Stockham passes).
+struct AxisPlan {
+  int n;
+  int npass;
+  int radix[kMaxPasses];
+};
+
+// Geometry of one patch scale (src/recon.jl:54-72), all 0-based.
+struct ScaleGeom {
+  int ps[3];        // clamped patch size
+  int ss[3];        // stride
+  int nsteps[3];    // cld(N - ps, ss)
+  int64_t Np;       // number of patches
+  int p;            // prod(ps)
+  int n;            // min(p, Nt): side of the Gram matrix
+  int L;            // max(p, Nt): contraction length of the Gram
+  bool tall;        // p >= Nt: Gram = P^H P (time x time); else P P^H (voxel x voxel)
+  bool partition;   // patches tile the volume exactly (no overlap, no gaps)
+  bool global;      // one patch covering the whole volume
+  int* d_starts;    // device: x-starts, y-starts, z-starts (nsteps+1 each)
+  // coverage ranges per dim for the gather recombine: for coordinate c in dim d,
+  // covering patch indices along d are [lo, hi] (inclusive); -1 if none
+  int* d_cover;     // device: per dim, 2*N[d] ints
+  std::vector<int> h_starts;
+};
+
+// Status helpers -------------------------------------------------------------
+struct Status {
+  int code = MSLR_OK;
+  std::string msg;
+};
+
+}  // namespace mslr
+
+#define MSLR_CUDA_TRY(expr)                                                        \
+  do {                                                                             \
+    cudaError_t _e = (expr);                                                       \
+    if (_e != cudaSuccess) {                                                       \
+      return ::mslr::fail(MSLR_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    }                                                                              \
+  } while (0)

@@ -1,0 +1,121 @@
+// internal.h — context structure and launcher declarations shared by the
+// translation units of libmslr.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mslr {
+
+// Thread-local error message of the last failing call (context-free calls).
+int fail(int code, const std::string& msg);
+const std::string& last_error_tls();
+
+// Device-side POGM scalar state (src/mirt_mod.jl:97-184 scalars).  Lives in
+// device memory so that one iteration can be captured in a CUDA graph and
+// replayed without host round trips.
+struct PogmState {
+  double told, sig, tnew;
+  double alpha, beta, gamma, zeta;
+  double restart_cutoff, bsig;
+  int iter, niter;
+  int flags;               // bit0: sigma-decrease test needed (bsig != 1)
+  int pad;
+  double red[4];           // last reductions: Σ Re(−g·Δu), ‖g‖², ‖Δu‖², Σ Re(g·gold)
+};
+
+// Per-scale SVST workspace layout (all patches of a scale share one layout).
+struct SvstWork {
+  int n = 0;                 // Gram side
+  int64_t np = 0;            // patches
+  cf* gram = nullptr;        // np * n * n   Gram, then Householder vectors, then W
+  cf* zv = nullptr;          // np * n * n   FP64 tridiagonal eigenvectors, then V (complex64)
+  double* aux = nullptr;     // np * n * n   FP64 scratch for the twisted factorisations
+  double* vecs = nullptr;    // np * 6 * n   d, e, tau(re,im), eigenvalues, h
+  int* rank = nullptr;       // np          number of singular values above β
+  cf* split_part = nullptr;  // nsplit * n * n partial Grams (split-K)
+  int nsplit = 1;
+};
+
+struct Ctx {
+  int N[3] = {0, 0, 0};
+  int Nc = 0, Nt = 0;
+  int64_t K = 0;
+  int Ns = 0;
+  int form = MSLR_FORM_PLAIN;
+  int64_t nvox = 0;
+  int device = 0;
+  std::vector<ScaleGeom> scales;
+  std::vector<double> lambdas;   // Ong–Lustig λ_k (scripts/reconstruct.jl:163-169)
+
+  // SENSE
+  AxisPlan plan[3];
+  cf* d_tw[3] = {nullptr, nullptr, nullptr};     // twiddles exp(-2πik/n)
+  cf* d_phase[3] = {nullptr, nullptr, nullptr};  // φ_d(k) = exp(2πi c(k-c)/n)
+  cf* d_mod[3] = {nullptr, nullptr, nullptr};    // m_d(j) = exp(2πi j c/n)
+  cf* d_smaps_mod = nullptr;   // (Nc, nvox) coil maps × input modulation
+  uint32_t* d_mask = nullptr;  // (Nt, nwords) sampling bitmasks
+  int nwords = 0;
+  int32_t* d_idx = nullptr;    // (Nt, K) 0-based
+  cf* d_ahy = nullptr;         // (Nt, nvox) A'y
+  cf* d_T = nullptr;           // (F, Nc, nvox) per-coil k-space of a chunk of frames
+  int F = 1;
+  bool bound = false;
+
+  // POGM
+  cf* d_U = nullptr;   // (Ns, Nt, nvox)
+  cf* d_Z = nullptr;   // (Ns, Nt, nvox) pre-prox iterate z_i
+  cf* d_G = nullptr;   // (Nt, nvox) gradient
+  cf* d_Gold = nullptr;  // (Nt, nvox) previous gradient (only when bsig != 1)
+  double* d_part = nullptr;   // reduction partials
+  int nred_blocks = 0;
+  PogmState* d_state = nullptr;
+  uint8_t* d_restarts = nullptr;  // niter+1
+  int restarts_cap = 0;
+  double* d_thr = nullptr;    // device threshold multiplier (ζ for POGM, β for standalone)
+  int32_t* d_err = nullptr;   // device error word
+  bool pogm_ready = false;
+
+  // SVST
+  std::vector<SvstWork> svw;   // one per scale (the plain form shares buffers across scales)
+  cf* d_pbuf = nullptr;        // per-patch output buffer for non-partition scales
+  size_t pbuf_elems = 0;
+  cf* d_img_tmp = nullptr;     // (Nt, nvox) out-of-place staging for in-place calls
+
+  size_t bytes = 0;
+  uint64_t launches = 0;   // kernels launched through this context
+  std::string err;
+};
+
+// ---- device memory helper -------------------------------------------------
+int dalloc(Ctx* c, void** p, size_t bytes);
+
+// ---- sense.cu ----------------------------------------------------------------
+int sense_setup_tables(Ctx* c);   // twiddles, phases, plans (create time)
+int sense_bind(Ctx* c, const cf* smaps, const cf* y, const int32_t* idx, int base,
+               cudaStream_t st);
+int sense_forward(Ctx* c, const cf* x, cf* y, cudaStream_t st);
+int sense_adjoint(Ctx* c, const cf* y, cf* x, cudaStream_t st);
+// g = A'(A Σ_k X_k − y) (subtract) or A'A Σ_k X_k
+int normal_op(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
+              cudaStream_t st);
+
+// ---- svst.cu -----------------------------------------------------------------
+int svst_setup(Ctx* c);   // workspaces (create time)
+// img_out = patchSVST(img_in) for scale s with threshold (*thr_dev) * lam
+int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_in, cf* img_out,
+               cudaStream_t st);
+int geom_build(const int N[3], int Nt, const int ps_in[3], const int ss_in[3], ScaleGeom* g);
+int geom_upload(ScaleGeom* g, const int N[3]);
+void geom_free(ScaleGeom* g);
+
+// ---- pogm.cu -----------------------------------------------------------------
+int pogm_setup(Ctx* c);
+int pogm_begin(Ctx* c, cf* X, int niter, double L, double cutoff, double bsig, cudaStream_t st);
+int pogm_step(Ctx* c, cf* X, cudaStream_t st);
+int init_x0(Ctx* c, cf* X, cudaStream_t st);
+int power_iter(Ctx* c, int niter, double tol, double* sigma1, int* iters, cudaStream_t st);
+int set_scalar(double* dst, double v, cudaStream_t st);
+
+}  // namespace mslr

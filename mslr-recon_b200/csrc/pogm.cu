@@ -1,0 +1,300 @@
+// pogm.cu — POGM with gradient restart and power iteration on sm_100a.
+//
+// pogm_mod (src/mirt_mod.jl:74-188) with mom=:pogm, μ=0, restart=:gr, as
+// driven by run_recon (scripts/reconstruct.jl:220-226).  run_recon's g_prox
+// writes into its argument (scripts/reconstruct.jl:196-202), so in the
+// reference xnew aliases znew; consequently Fgrad ≡ fgrad, ynew ≡ unew and
+// the β·α/ζold·(xold − zold) term is identically zero.  The recurrence run
+// here is therefore, per iteration i (t_0 = 1, u_0 = x_0):
+//
+//   g   = ∇f(x_{i-1})                         (the same for every scale)
+//   u_i = x_{i-1} − α g
+//   t_i = ½(1 + √(1 + 4 t²))  (8 t² at i = niter);  β = (t−1)/t_i;  γ = σ t/t_i
+//   z_i = u_i + β (u_i − u_{i-1}) + γ (u_i − x_{i-1});  ζ = α (1 + β + γ)
+//   x_i = prox_{ζ Σ λ_k ‖·‖_*}(z_i)          (per-scale patch SVST)
+//   restart if Σ Re(−g·(u_i − u_{i-1})) ≤ cutoff·‖g‖·‖u_i − u_{i-1}‖
+//     (src/mirt_mod.jl:26-29: unconjugated product, Float64 sum)
+//
+// One fused kernel produces u_i and z_i and the FP64 restart reductions in a
+// single pass over x, u and g; the scalar recurrence runs on the device so
+// that a whole iteration can be replayed from a CUDA graph.
+#include <cmath>
+
+#include "internal.h"
+
+namespace mslr {
+
+namespace {
+
+constexpr int kRedBlocks = 1184;  // 148 SMs × 8 — fixed so reductions are deterministic
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sh[i];
+  }
+  return r;  // valid in thread 0
+}
+
+// t, β, γ, ζ of the coming iteration (src/mirt_mod.jl:138-156).
+__global__ void k_pogm_prepare(PogmState* s, double* thr) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double told = s->told;
+  const double tnew = (s->iter == s->niter) ? 0.5 * (1.0 + sqrt(1.0 + 8.0 * told * told))
+                                            : 0.5 * (1.0 + sqrt(1.0 + 4.0 * told * told));
+  const double beta = (told - 1.0) / tnew;
+  const double gamma = s->sig * told / tnew;
+  s->tnew = tnew;
+  s->beta = beta;
+  s->gamma = gamma;
+  s->zeta = s->alpha * (1.0 + beta + gamma);
+  *thr = s->zeta;
+}
+
+// u ← x − α g;  z ← u + β(u − uold) + γ(u − x);  FP64 partial reductions.
+__global__ void __launch_bounds__(kRedThreads)
+    k_pogm_update(const cf* __restrict__ X, cf* __restrict__ U, const cf* __restrict__ G,
+                  cf* __restrict__ Gold, cf* __restrict__ Z, int64_t E, int ns,
+                  const PogmState* __restrict__ s, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const float alpha = (float)s->alpha, beta = (float)s->beta, gamma = (float)s->gamma;
+  const bool sigtest = (s->flags & 1) != 0;
+  double r_dot = 0.0, r_g2 = 0.0, r_d2 = 0.0, r_sig = 0.0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const cf g = G[e];
+    r_g2 += (double)g.x * g.x + (double)g.y * g.y;
+    if (sigtest) {
+      const cf go = Gold[e];
+      r_sig += (double)g.x * go.x - (double)g.y * go.y;
+      Gold[e] = g;
+    }
+    for (int k = 0; k < ns; ++k) {
+      const int64_t o = (int64_t)k * E + e;
+      const cf xo = X[o];
+      const cf uo = U[o];
+      const cf un = make_float2(xo.x - alpha * g.x, xo.y - alpha * g.y);
+      const cf du = csub(un, uo);
+      const cf zn = make_float2(un.x + beta * du.x + gamma * (un.x - xo.x),
+                                un.y + beta * du.y + gamma * (un.y - xo.y));
+      U[o] = un;
+      Z[o] = zn;
+      r_dot += -((double)g.x * du.x - (double)g.y * du.y);
+      r_d2 += (double)du.x * du.x + (double)du.y * du.y;
+    }
+  }
+  double v;
+  v = block_sum(r_dot, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 4 + 0] = v;
+  v = block_sum(r_g2, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 4 + 1] = v;
+  v = block_sum(r_d2, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 4 + 2] = v;
+  v = block_sum(r_sig, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 4 + 3] = v;
+}
+
+// Restart decision and t/σ update (src/mirt_mod.jl:163-184).
+__global__ void k_pogm_finish(PogmState* s, const double* __restrict__ part, int nblocks,
+                              int ns, uint8_t* restarts, int32_t* err) {
+  __shared__ double sh[32];
+  double acc[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int q = 0; q < 4; ++q) acc[q] += part[b * 4 + q];
+  double tot[4];
+  for (int q = 0; q < 4; ++q) tot[q] = block_sum(acc[q], sh);
+  if (threadIdx.x != 0) return;
+  const double dot = tot[0];
+  const double gnorm = sqrt((double)ns * tot[1]);   // ‖Fgrad‖ of the replicated 5-D gradient
+  const double dnorm = sqrt(tot[2]);
+  const double sigdot = (double)ns * tot[3];
+  for (int q = 0; q < 4; ++q) s->red[q] = tot[q];
+  if (!isfinite(dot) || !isfinite(gnorm) || !isfinite(dnorm)) atomicOr(err, 4);
+  int restart = 0;
+  double tnew = s->tnew;
+  if (dot <= s->restart_cutoff * gnorm * dnorm) {
+    tnew = 1.0;
+    s->sig = 1.0;
+    restart = 1;
+  } else if ((s->flags & 1) && sigdot < 0.0) {
+    s->sig = s->bsig * s->sig;
+  }
+  restarts[s->iter] = (uint8_t)restart;
+  s->told = tnew;
+  s->iter += 1;
+}
+
+__global__ void k_pogm_init(PogmState* s, double L, int niter, double cutoff, double bsig,
+                            uint8_t* restarts) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  s->told = 1.0;
+  s->sig = 1.0;
+  s->tnew = 1.0;
+  s->alpha = 1.0 / L;
+  s->beta = s->gamma = 0.0;
+  s->zeta = 1.0;
+  s->restart_cutoff = cutoff;
+  s->bsig = bsig;
+  s->iter = 1;
+  s->niter = niter;
+  s->flags = (bsig != 1.0) ? 1 : 0;
+  for (int q = 0; q < 4; ++q) s->red[q] = 0.0;
+  restarts[0] = 0;
+}
+
+__global__ void k_set_scalar(double* dst, double v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = v;
+}
+
+// ---- power iteration helpers ----------------------------------------------
+__global__ void k_fill_one(cf* x, int64_t E) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+       e += (int64_t)gridDim.x * blockDim.x)
+    x[e] = make_float2(1.f, 0.f);
+}
+
+// part[b] = (Σ Re(conj(x)·p), Σ|x|², Σ|p|²)
+__global__ void __launch_bounds__(kRedThreads)
+    k_dots(const cf* __restrict__ x, const cf* __restrict__ p, int64_t E, double* part) {
+  __shared__ double sh[32];
+  double a = 0, b = 0, c = 0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const cf u = x[e], v = p[e];
+    a += (double)u.x * v.x + (double)u.y * v.y;
+    b += (double)u.x * u.x + (double)u.y * u.y;
+    c += (double)v.x * v.x + (double)v.y * v.y;
+  }
+  double r;
+  r = block_sum(a, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 3 + 0] = r;
+  r = block_sum(b, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 3 + 1] = r;
+  r = block_sum(c, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 3 + 2] = r;
+}
+
+__global__ void k_scale_into(cf* __restrict__ x, const cf* __restrict__ p, float s, int64_t E) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+       e += (int64_t)gridDim.x * blockDim.x)
+    x[e] = cscale(p[e], s);
+}
+
+}  // namespace
+
+int set_scalar(double* dst, double v, cudaStream_t st) {
+  k_set_scalar<<<1, 32, 0, st>>>(dst, v);
+  MSLR_CUDA_TRY(cudaGetLastError());
+  return MSLR_OK;
+}
+
+int pogm_setup(Ctx* c) {
+  int rc;
+  const size_t E = (size_t)c->Nt * c->nvox;
+  if ((rc = dalloc(c, (void**)&c->d_U, (size_t)c->Ns * E * sizeof(cf)))) return rc;
+  if ((rc = dalloc(c, (void**)&c->d_Z, (size_t)c->Ns * E * sizeof(cf)))) return rc;
+  if ((rc = dalloc(c, (void**)&c->d_G, E * sizeof(cf)))) return rc;
+  if ((rc = dalloc(c, (void**)&c->d_part, (size_t)kRedBlocks * 4 * sizeof(double)))) return rc;
+  if ((rc = dalloc(c, (void**)&c->d_state, sizeof(PogmState)))) return rc;
+  c->nred_blocks = kRedBlocks;
+  return MSLR_OK;
+}
+
+int init_x0(Ctx* c, cf* X, cudaStream_t st) {
+  const size_t E = (size_t)c->Nt * c->nvox;
+  MSLR_CUDA_TRY(cudaMemcpyAsync(X, c->d_ahy, E * sizeof(cf), cudaMemcpyDeviceToDevice, st));
+  if (c->Ns > 1)
+    MSLR_CUDA_TRY(cudaMemsetAsync(X + E, 0, (size_t)(c->Ns - 1) * E * sizeof(cf), st));
+  return MSLR_OK;
+}
+
+int pogm_begin(Ctx* c, cf* X, int niter, double L, double cutoff, double bsig, cudaStream_t st) {
+  int rc;
+  const size_t E = (size_t)c->Nt * c->nvox;
+  if (niter + 1 > c->restarts_cap) {
+    if (c->d_restarts) cudaFree(c->d_restarts);
+    c->d_restarts = nullptr;
+    if ((rc = dalloc(c, (void**)&c->d_restarts, (size_t)niter + 1))) return rc;
+    c->restarts_cap = niter + 1;
+  }
+  MSLR_CUDA_TRY(cudaMemsetAsync(c->d_restarts, 0, (size_t)niter + 1, st));
+  if (bsig != 1.0) {
+    if (!c->d_Gold && (rc = dalloc(c, (void**)&c->d_Gold, E * sizeof(cf)))) return rc;
+    MSLR_CUDA_TRY(cudaMemsetAsync(c->d_Gold, 0, E * sizeof(cf), st));
+  }
+  // u_0 = x_0 (src/mirt_mod.jl:98)
+  MSLR_CUDA_TRY(cudaMemcpyAsync(c->d_U, X, (size_t)c->Ns * E * sizeof(cf),
+                                cudaMemcpyDeviceToDevice, st));
+  k_pogm_init<<<1, 32, 0, st>>>(c->d_state, L, niter, cutoff, bsig, c->d_restarts);
+  MSLR_CUDA_TRY(cudaGetLastError());
+  c->pogm_ready = true;
+  return MSLR_OK;
+}
+
+int pogm_step(Ctx* c, cf* X, cudaStream_t st) {
+  int rc;
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  // 1. g = A'(A Σ_k x_k − y)   (scripts/reconstruct.jl:180-183)
+  if ((rc = normal_op(c, X, c->Ns, E, c->d_G, true, st))) return rc;
+  // 2. momentum scalars, 3. fused u/z update + restart reductions
+  k_pogm_prepare<<<1, 32, 0, st>>>(c->d_state, c->d_thr);
+  k_pogm_update<<<kRedBlocks, kRedThreads, 0, st>>>(X, c->d_U, c->d_G, c->d_Gold, c->d_Z, E,
+                                                    c->Ns, c->d_state, c->d_part);
+  k_pogm_finish<<<1, kRedThreads, 0, st>>>(c->d_state, c->d_part, kRedBlocks, c->Ns,
+                                           c->d_restarts, c->d_err);
+  MSLR_CUDA_TRY(cudaGetLastError());
+  c->launches += 3;
+  // 4. x_i = g_prox(z_i, ζ): per-scale patch SVST with threshold ζ·λ_k
+  for (int k = 0; k < c->Ns; ++k) {
+    if ((rc = patch_svst(c, k, c->d_thr, c->lambdas[k], c->d_Z + k * E, X + k * E, st)))
+      return rc;
+  }
+  return MSLR_OK;
+}
+
+int power_iter(Ctx* c, int niter, double tol, double* sigma1, int* iters, cudaStream_t st) {
+  int rc;
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  cf* x = c->d_U;   // scratch: first scale slot of u
+  cf* p = c->d_G;
+  std::vector<double> h(kRedBlocks * 3);
+  auto dots = [&](double* out) -> int {
+    k_dots<<<kRedBlocks, kRedThreads, 0, st>>>(x, p, E, c->d_part);
+    MSLR_CUDA_TRY(cudaGetLastError());
+    MSLR_CUDA_TRY(cudaMemcpyAsync(h.data(), c->d_part, h.size() * sizeof(double),
+                                  cudaMemcpyDeviceToHost, st));
+    MSLR_CUDA_TRY(cudaStreamSynchronize(st));
+    out[0] = out[1] = out[2] = 0;
+    for (int b = 0; b < kRedBlocks; ++b)
+      for (int q = 0; q < 3; ++q) out[q] += h[b * 3 + q];
+    return MSLR_OK;
+  };
+  k_fill_one<<<kRedBlocks, kRedThreads, 0, st>>>(x, E);   // x0 = ones (src/mirt_mod.jl:219)
+  double ratio_old = INFINITY;
+  int it = 0;
+  double d[3];
+  for (it = 1; it <= niter; ++it) {
+    if ((rc = normal_op(c, x, 1, E, p, false, st))) return rc;   // p = A'A x
+    if ((rc = dots(d))) return rc;
+    // ‖Ax‖/‖x‖ with ‖Ax‖² = <x, A'A x>
+    const double ratio = std::sqrt(std::max(d[0], 0.0)) / std::sqrt(d[1]);
+    if (!std::isfinite(ratio)) return fail(MSLR_ERR_NONFINITE, "power iteration diverged");
+    if (std::fabs(ratio - ratio_old) / ratio < tol) break;
+    ratio_old = ratio;
+    // x = A'Ax / ‖A'Ax‖
+    k_scale_into<<<kRedBlocks, kRedThreads, 0, st>>>(x, p, (float)(1.0 / std::sqrt(d[2])), E);
+  }
+  if (iters) *iters = std::min(it, niter);
+  if ((rc = normal_op(c, x, 1, E, p, false, st))) return rc;
+  if ((rc = dots(d))) return rc;
+  *sigma1 = std::sqrt(std::max(d[0], 0.0)) / std::sqrt(d[1]);
+  return MSLR_OK;
+}
+
+}  // namespace mslr

@@ -1,0 +1,59 @@
+"""run_recon on in-memory arrays — the hot part of scripts/reconstruct.jl:59-263.
+
+File loading (scripts/reconstruct.jl:86-105) and saving (:241-262) are the
+caller's business; this module takes coil maps, sampled k-space and sample
+indices, builds the context, and runs POGM (mom=:pogm, restart=:gr) on the
+device.  It returns what run_recon saves, minus the files.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .context import MSLRContext
+
+
+def sos_normalize(smaps: np.ndarray) -> np.ndarray:
+    """scripts/reconstruct.jl:89: S ./ (sqrt(Σ_c |S_c|²) .+ eps(Float32))."""
+    sos = np.sqrt(np.sum(np.abs(smaps) ** 2, axis=0)).astype(np.float32)
+    return (smaps / (sos + np.finfo(np.float32).eps)[None]).astype(np.complex64)
+
+
+def run_recon(smaps, y, idx, patch_sizes, strides, niters: int, sigma1=None, form: str = "tuned",
+              index_base: int = 0, power_niter: int = 200, power_tol: float = 1e-6,
+              restart_cutoff: float = 0.0, bsig: float = 1.0, return_components: bool = True):
+    """Arguments are host numpy arrays or CUDA tensors in the layouts of
+    :mod:`context`.  ``sigma1=None`` runs the power iteration (as
+    σ1A_PRECOMPUTED = nothing, scripts/reconstruct.jl:152-158).
+
+    Returns a dict with X (Ns,Nt,Nz,Ny,Nx), X_recon, restarts, lambdas,
+    sigma1A and L, all on the host.
+    """
+    dev = torch.device("cuda")
+    smaps_t = torch.as_tensor(smaps).to(dev, torch.complex64).contiguous()
+    y_t = torch.as_tensor(y).to(dev, torch.complex64).contiguous()
+    idx_t = torch.as_tensor(idx).to(dev, torch.int32).contiguous()
+    Nc, Nz, Ny, Nx = smaps_t.shape
+    Nt, _, K = y_t.shape
+    with MSLRContext((Nx, Ny, Nz), Nc, Nt, K, patch_sizes, strides, form=form) as ctx:
+        ctx.bind(smaps_t, y_t, idx_t, index_base=index_base)
+        if sigma1 is None:
+            sigma1, _ = ctx.power_iter(power_niter, power_tol)
+        L = ctx.Ns * float(sigma1) ** 2
+        X = ctx.init_x0()
+        restarts = ctx.pogm_run(X, niters, L, restart_cutoff, bsig)
+        torch.cuda.synchronize()
+        out = {
+            "X_recon": X.sum(dim=0).cpu().numpy(),
+            "restarts": restarts,
+            "lambdas": list(ctx.lambdas),
+            "sigma1A": float(sigma1),
+            "L": L,
+            "Nscales": ctx.Ns,
+            "patch_sizes": ctx.patch_sizes,
+            "strides": ctx.strides,
+            "Niters": niters,
+        }
+        if return_components:
+            out["X"] = X.cpu().numpy()
+    return out

@@ -1,0 +1,489 @@
+"""CPU oracle for the MSLR POGM hot path — TEST INFRASTRUCTURE ONLY.
+
+This module restates, in numpy, the arithmetic of rextlfung/mslr-recon's
+per-iteration path so that the CUDA library can be checked against it.  It is
+imported only by ``tests/``, by ``__graft_entry__.smoke()`` and by the
+``cpu_baseline`` / ``--impl reference`` legs of ``bench.py``; the product path
+(``mslr-recon_b200``) never imports it and fails loudly when its CUDA library
+is missing.
+
+Parity status: UNPINNED.  The reference is Julia (FFTW / LAPACK / CUDA.jl) and
+ships no tests, golden vectors or fixtures; Julia is not installed here, so the
+reference itself cannot be run to pin this restatement.  The restatement is
+instead checked against known-answer properties of the mathematics (unitary
+SENSE adjointness, SVST of matrices with known SVD, patch extract/recombine
+identities, Ong–Lustig λ values) in ``tests/test_oracle.py``.
+
+Memory layouts follow the reference's column-major Julia arrays exactly, read
+as C-order numpy arrays with the axes reversed:
+
+=====================  ==========================  ==========================
+quantity               Julia (column-major)        numpy here (C-order)
+=====================  ==========================  ==========================
+image time series      (Nx, Ny, Nz, Nt)            (Nt, Nz, Ny, Nx)
+multi-scale X          (Nx, Ny, Nz, Nt, Ns)        (Ns, Nt, Nz, Ny, Nx)
+coil maps              (Nx, Ny, Nz, Nc)            (Nc, Nz, Ny, Nx)
+sampled k-space y      (K, Nc, Nt)                 (Nt, Nc, K)
+patch stack P          (p, Nt, Np)                 (Np, Nt, p)
+=====================  ==========================  ==========================
+
+Linear k-space indices are the reference's ``findall(vec(samp))`` minus one:
+ascending 0-based column-major indices ``x + Nx*(y + Ny*z)``, i.e. flat
+indices into a C-order ``(Nz, Ny, Nx)`` array.
+
+Every function cites the reference file:line it restates.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import Callable, List, Sequence
+
+import numpy as np
+import scipy.fft as sfft
+import scipy.linalg as sla
+
+SPATIAL_AXES = (-3, -2, -1)
+
+
+# ---------------------------------------------------------------------------
+# Patch geometry — src/recon.jl:53-78 (img2patches), :96-126 (patches2img)
+# ---------------------------------------------------------------------------
+def cld(a: int, b: int) -> int:
+    """Julia ``cld`` (ceiling division) for integers."""
+    return -((-a) // b)
+
+
+@dataclass(frozen=True)
+class PatchGeometry:
+    """Clamped-stride patch grid of one scale (src/recon.jl:57-75).
+
+    ``ps`` / ``ss`` / ``N`` are (x, y, z) triples.  ``starts[d]`` holds the
+    0-based start of every patch along dimension d; patch ``ip`` (0-based)
+    enumerates ix fastest, then iy, then iz (src/recon.jl:69).
+    """
+
+    N: tuple
+    ps: tuple
+    ss: tuple
+    nsteps: tuple
+    starts: tuple
+
+    @property
+    def Np(self) -> int:
+        return (self.nsteps[0] + 1) * (self.nsteps[1] + 1) * (self.nsteps[2] + 1)
+
+    @property
+    def p(self) -> int:
+        return self.ps[0] * self.ps[1] * self.ps[2]
+
+    def patch_start(self, ip: int) -> tuple:
+        nx, ny = self.nsteps[0] + 1, self.nsteps[1] + 1
+        ix = ip % nx
+        iy = (ip // nx) % ny
+        iz = ip // (nx * ny)
+        return (self.starts[0][ix], self.starts[1][iy], self.starts[2][iz])
+
+
+def patch_geometry(N: Sequence[int], patch_size: Sequence[int], stride_size: Sequence[int]) -> PatchGeometry:
+    """src/recon.jl:54-72: ``ps = min(ps, N)``, ``nsteps = cld(N-ps, ss)``,
+    ``start(i) = min(i*ss + 1, N - ps + 1)`` (1-based; returned 0-based)."""
+    N = tuple(int(v) for v in N)
+    ps = tuple(min(int(p), n) for p, n in zip(patch_size, N))
+    ss = tuple(int(s) for s in stride_size)
+    if any(s <= 0 for s in ss):
+        raise ValueError("strides must be positive")
+    nsteps = tuple(cld(n - p, s) for n, p, s in zip(N, ps, ss))
+    starts = tuple(
+        tuple(min(i * s, n - p) for i in range(ns + 1))
+        for n, p, s, ns in zip(N, ps, ss, nsteps)
+    )
+    return PatchGeometry(N=N, ps=ps, ss=ss, nsteps=nsteps, starts=starts)
+
+
+def img2patches(img: np.ndarray, patch_size, stride_size) -> np.ndarray:
+    """src/recon.jl:53-78.  ``img`` (Nt, Nz, Ny, Nx) -> P (Np, Nt, p)."""
+    Nt, Nz, Ny, Nx = img.shape
+    g = patch_geometry((Nx, Ny, Nz), patch_size, stride_size)
+    psx, psy, psz = g.ps
+    P = np.zeros((g.Np, Nt, g.p), dtype=img.dtype)
+    for ip in range(g.Np):
+        sx, sy, sz = g.patch_start(ip)
+        blk = img[:, sz:sz + psz, sy:sy + psy, sx:sx + psx]
+        P[ip] = blk.reshape(Nt, g.p)
+    return P
+
+
+def patches2img(P: np.ndarray, patch_size, stride_size, og_size) -> np.ndarray:
+    """src/recon.jl:96-126: sum patches in ascending ip, Float32 coverage
+    count, ``max(count, 1)``, divide."""
+    Np, Nt, p = P.shape
+    g = patch_geometry(og_size, patch_size, stride_size)
+    Nx, Ny, Nz = g.N
+    psx, psy, psz = g.ps
+    img = np.zeros((Nt, Nz, Ny, Nx), dtype=P.dtype)
+    count = np.zeros((Nz, Ny, Nx), dtype=np.float32)
+    for ip in range(Np):
+        sx, sy, sz = g.patch_start(ip)
+        img[:, sz:sz + psz, sy:sy + psy, sx:sx + psx] += P[ip].reshape(Nt, psz, psy, psx)
+        count[sz:sz + psz, sy:sy + psy, sx:sx + psx] += np.float32(1)
+    count = np.maximum(count, np.float32(1))
+    img /= count[None].astype(img.real.dtype)
+    return img
+
+
+def coverage_count(N, patch_size, stride_size) -> np.ndarray:
+    """Float32 coverage counts before the ``max(.,1)`` clamp
+    (src/recon.jl:113-121)."""
+    g = patch_geometry(N, patch_size, stride_size)
+    Nx, Ny, Nz = g.N
+    psx, psy, psz = g.ps
+    count = np.zeros((Nz, Ny, Nx), dtype=np.float32)
+    for ip in range(g.Np):
+        sx, sy, sz = g.patch_start(ip)
+        count[sz:sz + psz, sy:sy + psy, sx:sx + psx] += np.float32(1)
+    return count
+
+
+# ---------------------------------------------------------------------------
+# SVST — src/recon.jl:183-211, loops :217-269
+# ---------------------------------------------------------------------------
+def _svd(X: np.ndarray):
+    """gesdd with a gesvd fallback, as src/recon.jl:189-193."""
+    try:
+        return sla.svd(X, full_matrices=False, lapack_driver="gesdd", check_finite=False)
+    except (np.linalg.LinAlgError, ValueError):
+        return sla.svd(X, full_matrices=False, lapack_driver="gesvd", check_finite=False)
+
+
+def svst(X: np.ndarray, beta: float) -> np.ndarray:
+    """src/recon.jl:183-205: zero-norm skip, thin SVD, ``max(S - β, 0)``,
+    rebuild from the kept (s > 0) columns (CPU variant)."""
+    if np.linalg.norm(X) == 0:
+        return np.zeros_like(X)
+    U, S, Vt = _svd(X)
+    s = np.maximum(S - S.dtype.type(beta), 0)
+    keep = s > 0
+    if not keep.any():
+        return np.zeros_like(X)
+    return (U[:, keep] * s[keep]) @ Vt[keep, :]
+
+
+def patch_svst(img: np.ndarray, beta, patch_size, stride_size) -> np.ndarray:
+    """src/recon.jl:251-256 (global β) and :263-268 (per-patch λs).
+
+    ``img`` (Nt, Nz, Ny, Nx).  Each patch matrix is (p × Nt) in the
+    reference; here P[ip] is its transpose (Nt × p), and SVST commutes with
+    transposition, so ``svst(P[ip].T).T`` is applied.
+    """
+    Nt, Nz, Ny, Nx = img.shape
+    P = img2patches(img, patch_size, stride_size)
+    Np = P.shape[0]
+    betas = np.broadcast_to(np.asarray(beta, dtype=np.float64), (Np,))
+    for ip in range(Np):
+        P[ip] = svst(P[ip].T.copy(), float(betas[ip])).T
+    return patches2img(P, patch_size, stride_size, (Nx, Ny, Nz))
+
+
+def patch_nucnorm(P: np.ndarray) -> float:
+    """src/recon.jl:138-146: Σ over patches of Σ svdvals (Float64 sum)."""
+    total = 0.0
+    for ip in range(P.shape[0]):
+        total += float(np.sum(sla.svdvals(P[ip], check_finite=False), dtype=np.float64))
+    return total
+
+
+# ---------------------------------------------------------------------------
+# SENSE operator — src/sense_gpu.jl:51-101 (convention of MIRT.Asense with
+# fft_forward=true, unitary=true).  The adjoint is the exact adjoint of the
+# forward (scale·bfft), i.e. MIRT's unitary pair.
+# ---------------------------------------------------------------------------
+def _fftc(x, workers):
+    return sfft.fftshift(sfft.fftn(sfft.ifftshift(x, axes=SPATIAL_AXES), axes=SPATIAL_AXES,
+                                    workers=workers), axes=SPATIAL_AXES)
+
+
+def _bfftc(k, workers):
+    """Exact adjoint of :func:`_fftc`: fftshift(bfft(ifftshift(k))).  The
+    reference writes ifftshift(ifft(fftshift(.))) (src/sense_gpu.jl:93), which
+    is the same map for the even sizes it is used with."""
+    n = int(np.prod(k.shape[-3:]))
+    # unnormalised inverse: ifft * n
+    return sfft.fftshift(sfft.ifftn(sfft.ifftshift(k, axes=SPATIAL_AXES), axes=SPATIAL_AXES,
+                                    workers=workers), axes=SPATIAL_AXES) * n
+
+
+def sense_forward_frame(x: np.ndarray, smaps: np.ndarray, idx: np.ndarray, workers: int = -1) -> np.ndarray:
+    """src/sense_gpu.jl:71-81: ``scale·fftshift(fft(ifftshift(S.*x)))[idx, :]``.
+
+    x (Nz, Ny, Nx); smaps (Nc, Nz, Ny, Nx); idx 0-based ascending (K,).
+    Returns (Nc, K)."""
+    Nc = smaps.shape[0]
+    n = x.size
+    scale = 1.0 / math.sqrt(n)
+    kc = _fftc(smaps * x[None], workers) * scale
+    return kc.reshape(Nc, -1)[:, idx]
+
+
+def sense_adjoint_frame(y: np.ndarray, smaps: np.ndarray, idx: np.ndarray, workers: int = -1) -> np.ndarray:
+    """Exact adjoint of :func:`sense_forward_frame` (src/sense_gpu.jl:84-101
+    with the unitary ``scale·bfft`` inverse).  y (Nc, K) -> (Nz, Ny, Nx)."""
+    Nc, Nz, Ny, Nx = smaps.shape
+    n = Nx * Ny * Nz
+    scale = 1.0 / math.sqrt(n)
+    full = np.zeros((Nc, n), dtype=np.result_type(y.dtype, smaps.dtype))
+    full[:, idx] = y
+    xc = _bfftc(full.reshape(Nc, Nz, Ny, Nx), workers) * scale
+    return np.sum(np.conj(smaps) * xc, axis=0)
+
+
+def sense_forward(x: np.ndarray, smaps: np.ndarray, idx: np.ndarray, workers: int = -1) -> np.ndarray:
+    """Block-diagonal over frames (scripts/reconstruct.jl:142-147).
+    x (Nt, Nz, Ny, Nx); idx (Nt, K) -> y (Nt, Nc, K)."""
+    return np.stack([sense_forward_frame(x[t], smaps, idx[t], workers) for t in range(x.shape[0])])
+
+
+def sense_adjoint(y: np.ndarray, smaps: np.ndarray, idx: np.ndarray, workers: int = -1) -> np.ndarray:
+    return np.stack([sense_adjoint_frame(y[t], smaps, idx[t], workers) for t in range(y.shape[0])])
+
+
+def normal_op(x: np.ndarray, smaps: np.ndarray, idx: np.ndarray, workers: int = -1) -> np.ndarray:
+    """A'A x per frame (no data term)."""
+    return sense_adjoint(sense_forward(x, smaps, idx, workers), smaps, idx, workers)
+
+
+# ---------------------------------------------------------------------------
+# POGM — src/mirt_mod.jl:26-29 (_gr_restart), :74-188 (pogm_mod)
+# ---------------------------------------------------------------------------
+def _gr_restart(Fgrad, ynew_yold, restart_cutoff) -> bool:
+    """src/mirt_mod.jl:26-29: ``sum(Float64, real(-Fgrad .* ynew_yold)) <=
+    cutoff * norm(Fgrad) * norm(ynew_yold)`` — an unconjugated product."""
+    lhs = float(np.sum(np.real(-Fgrad * ynew_yold), dtype=np.float64))
+    rhs = restart_cutoff * float(np.linalg.norm(Fgrad)) * float(np.linalg.norm(ynew_yold))
+    return lhs <= rhs
+
+
+def pogm_mod(x0, Fcost: Callable, f_grad: Callable, f_L: float, *, f_mu: float = 0.0,
+             mom: str = "pogm", restart: str = "gr", restart_cutoff: float = 0.0,
+             bsig: float = 1.0, niter: int = 10,
+             g_prox: Callable = lambda z, c: z,
+             fun: Callable = lambda it, xk, yk, r: None,
+             iter_callback: Callable | None = None):
+    """Line-by-line restatement of src/mirt_mod.jl:74-188.
+
+    Object identity is preserved on purpose: when ``g_prox`` mutates and
+    returns its argument (as the reference's g_prox does,
+    scripts/reconstruct.jl:196-202), ``xnew is znew`` and the
+    ``β·α/ζold·(xold − zold)`` term vanishes exactly as in the reference.
+    ``iter_callback(iter, xnew, is_restart)`` is an oracle-only hook used by the
+    per-iteration parity tests.
+    """
+    if mom not in ("pgm", "fpgm", "pogm"):
+        raise ValueError(f"mom={mom}")
+    if restart not in ("none", "gr", "fr"):
+        raise ValueError(f"restart={restart}")
+    if f_L < 0 or f_mu < 0 or bsig < 0 or not abs(restart_cutoff) < 1:
+        raise ValueError("bad pogm_mod argument")
+    L = f_L
+    mu = f_mu
+    q = mu / L
+    told = 1.0
+    sig = 1.0
+    zetaold = 1.0
+    xold = x0
+    yold = x0
+    uold = x0
+    zold = x0
+    Fcostold = Fcost(x0)
+    Fgradold = np.zeros(np.shape(x0))
+    out = [None] * (niter + 1)
+    out[0] = fun(0, x0, x0, False)
+    xnew = ynew = None
+    for it in range(1, niter + 1):
+        alpha = 2 / (L + mu) if (mom == "pgm" and mu != 0) else 1 / L
+        fgrad = f_grad(xold)
+        is_restart = False
+        if mom in ("pgm", "fpgm"):
+            ynew = g_prox(xold - alpha * fgrad, alpha)
+            Fgrad = -(1 / alpha) * (ynew - xold)
+            Fcostnew = Fcost(ynew)
+            if restart != "none":
+                if (restart == "fr" and Fcostnew > Fcostold) or \
+                   (restart == "gr" and _gr_restart(Fgrad, ynew - yold, restart_cutoff)):
+                    told = 1.0
+                    is_restart = True
+                Fcostold = Fcostnew
+        else:
+            unew = xold - alpha * fgrad
+        if mom == "fpgm" and mu != 0:
+            beta = (1 - math.sqrt(q)) / (1 + math.sqrt(q))
+        elif mom == "pogm" and mu != 0:
+            beta = (2 + q - math.sqrt(q ** 2 + 8 * q)) ** 2 / 4 / (1 - q)
+        elif mom != "pgm":
+            if mom == "pogm" and it == niter:
+                tnew = 0.5 * (1 + math.sqrt(1 + 8 * told ** 2))
+            else:
+                tnew = 0.5 * (1 + math.sqrt(1 + 4 * told ** 2))
+            beta = (told - 1) / tnew
+        if mom == "pgm":
+            xnew = ynew
+        elif mom == "fpgm":
+            xnew = ynew + beta * (ynew - yold)
+        else:
+            gamma = (2 + q - math.sqrt(q ** 2 + 8 * q)) / 2 if mu != 0 else sig * told / tnew
+            znew = unew + beta * (unew - uold) + gamma * (unew - xold) \
+                - beta * alpha / zetaold * (xold - zold)
+            zetanew = alpha * (1 + beta + gamma)
+            xnew = g_prox(znew, zetanew)
+            Fgrad = fgrad - (1 / zetanew) * (xnew - znew)
+            ynew = xold - alpha * Fgrad
+            Fcostnew = Fcost(xnew)
+            if restart != "none":
+                if (restart == "fr" and Fcostnew > Fcostold) or \
+                   (restart == "gr" and _gr_restart(Fgrad, ynew - yold, restart_cutoff)):
+                    tnew = 1.0
+                    sig = 1.0
+                    is_restart = True
+                elif float(np.sum(np.real(Fgrad * Fgradold), dtype=np.float64)) < 0:
+                    sig = bsig * sig
+                Fcostold = Fcostnew
+                Fgradold = Fgrad
+            uold = unew
+            zold = znew
+            zetaold = zetanew
+        out[it] = fun(it, xnew, ynew, is_restart)
+        if iter_callback is not None:
+            iter_callback(it, xnew, is_restart)
+        xold = xnew
+        yold = ynew
+        if mom != "pgm" and mu == 0:
+            told = tnew
+    return (xnew if mom == "pogm" else ynew), out
+
+
+# ---------------------------------------------------------------------------
+# Power iteration — src/mirt_mod.jl:215-238
+# ---------------------------------------------------------------------------
+def poweriter_mod(Aop: Callable, Aadj: Callable, x0: np.ndarray, niter: int = 200,
+                  tol: float = 1e-6):
+    """src/mirt_mod.jl:215-238 with ``x0 = ones``.  Returns (x, σ1)."""
+    x = x0.copy()
+    ratio_old = math.inf
+    for _ in range(niter):
+        Ax = Aop(x)
+        ratio = float(np.linalg.norm(Ax)) / float(np.linalg.norm(x))
+        if abs(ratio - ratio_old) / ratio < tol:
+            break
+        ratio_old = ratio
+        x = Aadj(Ax)
+        x = x / np.linalg.norm(x)
+    return x, float(np.linalg.norm(Aop(x))) / float(np.linalg.norm(x))
+
+
+# ---------------------------------------------------------------------------
+# λ_k and L — scripts/reconstruct.jl:159, :163-169
+# ---------------------------------------------------------------------------
+def ong_lustig_lambdas(N, Nt, patch_sizes) -> List[float]:
+    """scripts/reconstruct.jl:163-169 (uses the *unclamped* patch sizes)."""
+    nvox = int(np.prod(N))
+    out = []
+    for ps in patch_sizes:
+        p = int(np.prod(ps))
+        out.append(math.sqrt(p) + math.sqrt(Nt) + math.sqrt(math.log(nvox * Nt / max(p, Nt))))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# run_recon's closures — scripts/reconstruct.jl:174-214, pogm call :220-226
+# ---------------------------------------------------------------------------
+@dataclass
+class ReconProblem:
+    smaps: np.ndarray          # (Nc, Nz, Ny, Nx), SOS-normalised
+    idx: np.ndarray            # (Nt, K) 0-based
+    y: np.ndarray              # (Nt, Nc, K)
+    patch_sizes: list
+    strides: list
+    sigma1: float = 1.0
+    workers: int = -1
+
+    @property
+    def N(self):
+        Nc, Nz, Ny, Nx = self.smaps.shape
+        return (Nx, Ny, Nz)
+
+    @property
+    def Nt(self):
+        return self.y.shape[0]
+
+    @property
+    def Ns(self):
+        return len(self.patch_sizes)
+
+    def lambdas(self):
+        return ong_lustig_lambdas(self.N, self.Nt, self.patch_sizes)
+
+    def lipschitz(self):
+        return self.Ns * self.sigma1 ** 2
+
+
+def run_recon_arrays(prob: ReconProblem, niters: int, dtype=np.complex128, log_costs: bool = False,
+                     iter_callback=None, restart_cutoff: float = 0.0, bsig: float = 1.0):
+    """The hot loop of scripts/reconstruct.jl:174-226 on in-memory arrays.
+
+    ``dtype=np.complex128`` is the FP64 oracle; ``np.complex64`` mimics the
+    reference CPU precision.  Returns (X, restarts, dc_costs, reg_costs);
+    the cost lists are empty unless ``log_costs``.
+    """
+    Nx, Ny, Nz = prob.N
+    Nt, Ns = prob.Nt, prob.Ns
+    smaps = prob.smaps.astype(dtype)
+    y = prob.y.astype(dtype)
+    idx = prob.idx
+    lam = prob.lambdas()
+    L = prob.lipschitz()
+    w = prob.workers
+
+    def image_sum(X):
+        return X.sum(axis=0)
+
+    def dc_cost(X):
+        r = sense_forward(image_sum(X), smaps, idx, w) - y
+        return 0.5 * float(np.linalg.norm(r)) ** 2
+
+    def dc_cost_grad(X):
+        g = sense_adjoint(sense_forward(image_sum(X), smaps, idx, w) - y, smaps, idx, w)
+        return np.broadcast_to(g[None], (Ns,) + g.shape).astype(dtype, copy=True)
+
+    def reg_cost(X):
+        return sum(lam[k] * patch_nucnorm(img2patches(X[k], prob.patch_sizes[k], prob.strides[k]))
+                   for k in range(Ns))
+
+    def g_prox(X, c):
+        for k in range(Ns):
+            X[k] = patch_svst(X[k], c * lam[k], prob.patch_sizes[k], prob.strides[k])
+        return X
+
+    restarts = []
+    dcs, regs = [], []
+
+    def logger(it, xk, yk, is_restart):
+        restarts.append(bool(is_restart))
+        if log_costs:
+            dcs.append(dc_cost(xk))
+            regs.append(reg_cost(xk))
+        return None
+
+    X0 = np.zeros((Ns, Nt, Nz, Ny, Nx), dtype=dtype)
+    X0[0] = sense_adjoint(y, smaps, idx, w)
+    Xf, _ = pogm_mod(X0, (lambda X: 0.0), dc_cost_grad, L, mom="pogm", niter=niters,
+                     g_prox=g_prox, fun=logger, iter_callback=iter_callback,
+                     restart_cutoff=restart_cutoff, bsig=bsig)
+    return Xf, restarts, dcs, regs
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    """Relative Frobenius error ‖a − b‖ / ‖b‖ (FP64 accumulation)."""
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)

@@ -1,0 +1,219 @@
+"""GPU parity tests: every kernel path through the C ABI against the CPU
+oracle / the committed golden fixtures.
+
+Tolerances: patch indexing and masks are integer work and must be bit-exact;
+floating-point results must match the FP64 oracle to a relative Frobenius
+error of 1e-4 (the bound stated for the POGM iterate), with tighter bounds
+where single FP32 operations are involved.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mslr_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "golden_small.npz")
+PATCHES = [[8, 6, 4], [4, 3, 2], [3, 3, 3]]
+STRIDES = [[8, 6, 4], [4, 3, 2], [2, 2, 2]]
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+@pytest.fixture(scope="module")
+def M():
+    import mslr_recon_b200 as M
+    return M
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return dict(np.load(GOLD))
+
+
+def dev(torch, a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    elif t.is_complex():
+        t = t.to(torch.complex64)
+    return t.cuda()
+
+
+def rel(a, b):
+    return O.rel_err(a, b)
+
+
+# --- patch operators: bit-exact indexing -------------------------------------
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_img2patches_bit_exact(torch, M, gold, k):
+    x = gold["x"].astype(np.complex64)
+    P = M.img2patches(dev(torch, x), PATCHES[k], STRIDES[k]).cpu().numpy()
+    ref = O.img2patches(x, PATCHES[k], STRIDES[k])
+    assert P.shape == ref.shape
+    assert np.array_equal(P, ref)
+
+
+@pytest.mark.parametrize("N,ps,ss", [((13, 7, 5), (4, 4, 4), (3, 2, 4)), ((10, 1, 1), (2, 1, 1), (4, 1, 1)),
+                                     ((9, 9, 9), (3, 3, 3), (3, 3, 3)), ((11, 6, 4), (20, 3, 2), (5, 1, 1))])
+def test_recombine_matches_reference_order(torch, M, N, ps, ss):
+    rng = np.random.default_rng(11)
+    Nt = 5
+    g = O.patch_geometry(N, ps, ss)
+    P = (rng.standard_normal((g.Np, Nt, g.p)) + 1j * rng.standard_normal((g.Np, Nt, g.p))).astype(np.complex64)
+    out = M.patches2img(dev(torch, P), ps, ss, N).cpu().numpy()
+    ref = O.patches2img(P, ps, ss, N)   # float32 sums in ascending ip, same as the kernel
+    np.testing.assert_array_equal(out, ref)
+
+
+# --- SVST ------------------------------------------------------------------------
+@pytest.mark.parametrize("m,n,batch", [(40, 12, 5), (12, 40, 5), (216, 64, 7), (64, 216, 3), (1000, 300, 2),
+                                       (1, 30, 4), (30, 1, 4)])
+def test_svst_batch_vs_oracle(torch, M, m, n, batch):
+    rng = np.random.default_rng(m * 1000 + n)
+    X = (rng.standard_normal((batch, m, n)) + 1j * rng.standard_normal((batch, m, n))).astype(np.complex64)
+    # low-rank + noise so that thresholds land inside the spectrum
+    r = min(4, m, n)
+    for b in range(batch):
+        U = rng.standard_normal((m, r)) + 1j * rng.standard_normal((m, r))
+        V = rng.standard_normal((r, n)) + 1j * rng.standard_normal((r, n))
+        X[b] += (3.0 * U @ V).astype(np.complex64)
+    sv = [np.linalg.svd(X[b], compute_uv=False) for b in range(batch)]
+    betas = [float(np.median(s)) for s in sv]
+    betas[0] = 0.0
+    if batch > 2:
+        X[2] = 0
+        betas[2] = 1.0
+    cm = np.ascontiguousarray(np.transpose(X, (0, 2, 1)))   # column-major storage
+    out = M.svst_batch(dev(torch, cm), m, n, betas).cpu().numpy()
+    out = np.transpose(out, (0, 2, 1))
+    for b in range(batch):
+        ref = O.svst(X[b].astype(np.complex128), betas[b])
+        if np.linalg.norm(ref) == 0:
+            assert np.all(out[b] == 0)
+        else:
+            assert rel(out[b], ref) < 2e-5, (b, rel(out[b], ref))
+
+
+def test_svst_single_matrix(torch, M):
+    rng = np.random.default_rng(12)
+    X = (rng.standard_normal((50, 20)) + 1j * rng.standard_normal((50, 20))).astype(np.complex64)
+    out = M.SVST(dev(torch, X), 4.0).cpu().numpy()
+    assert rel(out, O.svst(X.astype(np.complex128), 4.0)) < 2e-5
+
+
+@pytest.mark.parametrize("k", [0, 1, 2])
+def test_patch_svst_golden(torch, M, gold, k):
+    out = M.patchSVST(dev(torch, gold["x"]), 3.0, PATCHES[k], STRIDES[k]).cpu().numpy()
+    assert rel(out, gold[f"svst{k}"]) < 2e-5
+
+
+# --- SENSE -------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def gctx(torch, M, gold):
+    Nt, Nc, K = gold["y"].shape
+    ctx = M.MSLRContext((8, 6, 4), Nc, Nt, K, PATCHES, STRIDES, form="plain")
+    ctx.bind(dev(torch, gold["smaps"]), dev(torch, gold["y"]), dev(torch, gold["idx"], torch.int32))
+    yield ctx
+    ctx.close()
+
+
+def test_sense_forward_golden(torch, gctx, gold):
+    y = gctx.forward(dev(torch, gold["x"])).cpu().numpy()
+    assert rel(y, gold["Ax"]) < 1e-5
+
+
+def test_sense_adjoint_golden(torch, gctx, gold):
+    x = gctx.adjoint(dev(torch, gold["y"])).cpu().numpy()
+    assert rel(x, gold["AHy"]) < 1e-5
+
+
+def test_normal_op_matches_forward_adjoint(torch, gctx, gold):
+    X = np.stack([gold["x"], 0.5 * gold["x"]]).astype(np.complex64)
+    g = gctx.normal(dev(torch, X)).cpu().numpy()
+    xs = X.astype(np.complex128).sum(0)
+    smaps, idx = gold["smaps"], gold["idx"]
+    ref = O.sense_adjoint(O.sense_forward(xs, smaps, idx) - gold["y"], smaps, idx)
+    assert rel(g, ref) < 1e-5
+
+
+def test_patch_svst_context_golden(torch, gctx, gold):
+    for k in range(3):
+        out = gctx.patch_svst(k, 3.0, dev(torch, gold["x"])).cpu().numpy()
+        assert rel(out, gold[f"svst{k}"]) < 2e-5, k
+
+
+# --- POGM ---------------------------------------------------------------------------
+def test_pogm_trajectory_golden(torch, gctx, gold):
+    X = gctx.init_x0()
+    traj = gold["traj"]
+    niter = traj.shape[0]
+    gctx.pogm_begin(X, niter, L=3.0)
+    errs = []
+    for i in range(niter):
+        gctx.pogm_step(X)
+        errs.append(rel(X.cpu().numpy(), traj[i]))
+    assert max(errs) < 1e-4, errs
+    assert gctx.pogm_restarts() == [bool(v) for v in gold["restarts"]]
+
+
+def test_power_iteration(torch, gctx, gold):
+    s1, it = gctx.power_iter(200, 1e-6)
+    smaps, idx = gold["smaps"], gold["idx"]
+    _, ref = O.poweriter_mod(lambda v: O.sense_forward(v, smaps, idx),
+                             lambda v: O.sense_adjoint(v, smaps, idx),
+                             np.ones(gold["x"].shape, complex), niter=200, tol=1e-6)
+    assert s1 == pytest.approx(ref, rel=1e-4)
+
+
+def test_small_workload_per_iteration_parity(torch, M, small_problem):
+    """The small workload (32x32x24, 8 coils, Nt=64, one 6^3 scale with
+    clamped edge patches, 20 iterations): X after every iteration within 1e-4
+    of the FP64 oracle, identical restart flags."""
+    pb = small_problem
+    Nt, Nc, K = pb["y"].shape
+    niter = pb["niters"]
+    prob = O.ReconProblem(smaps=pb["smaps"].astype(np.complex128), idx=pb["idx"],
+                          y=pb["y"].astype(np.complex128), patch_sizes=pb["patch_sizes"],
+                          strides=pb["strides"], sigma1=1.0)
+    traj = []
+    _, restarts, _, _ = O.run_recon_arrays(prob, niter, iter_callback=lambda it, xk, r: traj.append(xk.copy()))
+    for form in ("plain", "tuned"):
+        with M.MSLRContext(pb["N"], Nc, Nt, K, pb["patch_sizes"], pb["strides"], form=form) as ctx:
+            ctx.bind(dev(torch, pb["smaps"]), dev(torch, pb["y"]), dev(torch, pb["idx"], torch.int32))
+            X = ctx.init_x0()
+            ctx.pogm_begin(X, niter, L=1.0)
+            errs = []
+            for i in range(niter):
+                ctx.pogm_step(X)
+                errs.append(rel(X.cpu().numpy(), traj[i]))
+            assert max(errs) < 1e-4, (form, errs)
+            assert ctx.pogm_restarts() == restarts, form
+
+
+# --- errors -------------------------------------------------------------------------
+def test_bad_indices_rejected(torch, M, gold):
+    Nt, Nc, K = gold["y"].shape
+    with M.MSLRContext((8, 6, 4), Nc, Nt, K, PATCHES[:1], STRIDES[:1]) as ctx:
+        idx = gold["idx"].copy()
+        idx[0, 3] = idx[0, 2]   # duplicate -> not strictly ascending
+        with pytest.raises(ValueError, match="ascending"):
+            ctx.bind(dev(torch, gold["smaps"]), dev(torch, gold["y"]), dev(torch, idx, torch.int32))
+        idx = gold["idx"].copy()
+        idx[1, -1] = 8 * 6 * 4
+        with pytest.raises(ValueError, match="range"):
+            ctx.bind(dev(torch, gold["smaps"]), dev(torch, gold["y"]), dev(torch, idx, torch.int32))
+
+
+def test_state_errors(torch, M, gold):
+    Nt, Nc, K = gold["y"].shape
+    with M.MSLRContext((8, 6, 4), Nc, Nt, K, PATCHES[:1], STRIDES[:1]) as ctx:
+        with pytest.raises(M.MSLRError, match="bind"):
+            ctx.forward(dev(torch, gold["x"]))
