@@ -41,6 +41,7 @@ def load_problem(name: str, seed_offset: int = 0):
     spec = importlib.util.spec_from_file_location("mslr_synth_bench",
                                                   os.path.join(ROOT, "mslr-recon_b200", "synth.py"))
     S = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = S
     spec.loader.exec_module(S)
     import dataclasses
     cfg = dataclasses.replace(S.CONFIGS[name], seed=S.CONFIGS[name].seed + seed_offset)

@@ -128,7 +128,11 @@ def patches2img(P: np.ndarray, patch_size, stride_size, og_size) -> np.ndarray:
         img[:, sz:sz + psz, sy:sy + psy, sx:sx + psx] += P[ip].reshape(Nt, psz, psy, psx)
         count[sz:sz + psz, sy:sy + psy, sx:sx + psx] += np.float32(1)
     count = np.maximum(count, np.float32(1))
-    img /= count[None].astype(img.real.dtype)
+    # Julia's ComplexF32 ./ Float32 divides the real and imaginary parts
+    # separately (not a complex division)
+    c = count[None].astype(img.real.dtype)
+    img.real /= c
+    img.imag /= c
     return img
 
 

@@ -86,7 +86,7 @@ def test_svst_batch_vs_oracle(torch, M, m, n, batch):
         V = rng.standard_normal((r, n)) + 1j * rng.standard_normal((r, n))
         X[b] += (3.0 * U @ V).astype(np.complex64)
     sv = [np.linalg.svd(X[b], compute_uv=False) for b in range(batch)]
-    betas = [float(np.median(s)) for s in sv]
+    betas = [0.9 * float(np.median(s)) for s in sv]
     betas[0] = 0.0
     if batch > 2:
         X[2] = 0
