@@ -96,6 +96,26 @@ int mslr_svst_batch(int32_t m, int32_t n, int32_t batch, const double* betas,
                     const void* in, void* out, void* workspace, size_t workspace_bytes,
                     int32_t form, void* stream);
 
+/* Size of the fixed scratch array behind mslr_svst_batch_noalloc (16 MiB). */
+#define MSLR_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+
+/* Batched SVST that allocates nothing.  No counterpart in the reference: it
+ * exists for callers that cannot call cudaMalloc — e.g. a host framework
+ * whose memory pool owns the device (Julia's CUDA.jl or PyTorch's caching
+ * allocator) and must not have a library allocate behind the pool, or a
+ * real-time pipeline running on a fixed memory plan.  Same arguments and
+ * results as mslr_svst_batch, but the scratch is a file-scope device array
+ * of MSLR_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+ * until the process exits.  A batch needing more scratch than that
+ * (mslr_svst_batch_workspace reports the need) is rejected with
+ * MSLR_ERR_ARG.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  All calls share the one array, so calls
+ * that overlap on the GPU (different streams, or different host threads
+ * without ordering) race and corrupt each other's results. */
+int mslr_svst_batch_noalloc(int32_t m, int32_t n, int32_t batch, const double* betas,
+                            const void* in, void* out, void* stream);
+
 /* ------------------------------------------------------------------------
  * Reconstruction context — the state run_recon builds
  * (scripts/reconstruct.jl:133-214) for Ns scales of patch sizes/strides.

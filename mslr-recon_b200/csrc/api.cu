@@ -35,6 +35,8 @@ int patches_op(const int N[3], int Nt, const int ps[3], const int ss[3], const c
 size_t svst_batch_bytes(int mrows, int ncols, int batch);
 int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* in, cf* out,
                void* ws, size_t ws_bytes, cudaStream_t st);
+int svst_batch_noalloc(int mrows, int ncols, int batch, const double* betas, const cf* in, cf* out,
+                       cudaStream_t st);
 
 static void free_ctx(mslr_ctx* c) {
   void* ptrs[] = {c->d_tw[0], c->d_tw[1], c->d_tw[2], c->d_phase[0], c->d_phase[1], c->d_phase[2],
@@ -136,6 +138,18 @@ int mslr_svst_batch(int32_t m, int32_t n, int32_t batch, const double* betas, co
   (void)form;
   return svst_batch(m, n, batch, betas, reinterpret_cast<const cf*>(in), reinterpret_cast<cf*>(out),
                     workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mslr_svst_batch_noalloc(int32_t m, int32_t n, int32_t batch, const double* betas,
+                            const void* in, void* out, void* stream) {
+  if (m <= 0 || n <= 0 || batch <= 0 || !betas || !in || !out)
+    return fail(MSLR_ERR_ARG, "bad argument");
+  if (std::min(m, n) > 1024) return fail(MSLR_ERR_UNSUPPORTED, "min(m, n) must be <= 1024");
+  for (int b = 0; b < batch; ++b)
+    if (!(betas[b] >= 0.0) || !std::isfinite(betas[b]))
+      return fail(MSLR_ERR_ARG, "thresholds must be finite and non-negative");
+  return svst_batch_noalloc(m, n, batch, betas, reinterpret_cast<const cf*>(in),
+                            reinterpret_cast<cf*>(out), reinterpret_cast<cudaStream_t>(stream));
 }
 
 int mslr_create(const int32_t N[3], int32_t Nc, int32_t Nt, int64_t K, int32_t n_scales,

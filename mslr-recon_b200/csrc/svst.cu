@@ -25,6 +25,7 @@
 // count, clamped to 1 (src/recon.jl:113-124).
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "internal.h"
 
@@ -957,6 +958,51 @@ int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* i
     src = stage;
   }
   return svst_core(src, m, batch, w, 1, d_beta, 1, 1.0, out, 1, st, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Batched SVST without any allocation, for callers that cannot call
+// cudaMalloc (see mslr_svst_batch_noalloc in include/mslr.h).  Its scratch is
+// this file-scope device array: every GPU that loads the library holds it
+// until the process exits, and all calls share it.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[MSLR_NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch, looked up once per device.  In host
+// code the symbol name is only a host-side stand-in, so the kernels must be
+// given the address that cudaGetSymbolAddress returns for the current device.
+static void* g_noalloc_addr[64];
+static std::mutex g_noalloc_mu;
+
+int svst_batch_noalloc(int mrows, int ncols, int batch, const double* betas, const cf* in, cf* out,
+                       cudaStream_t st) {
+  const size_t need = svst_batch_bytes(mrows, ncols, batch);
+  if (need > (size_t)MSLR_NOALLOC_SCRATCH_BYTES)
+    return fail(MSLR_ERR_ARG,
+                "mslr_svst_batch_noalloc: this batch needs " + std::to_string(need) +
+                    " bytes of scratch, more than the fixed " +
+                    std::to_string((size_t)MSLR_NOALLOC_SCRATCH_BYTES) +
+                    " bytes; use mslr_svst_batch with a caller workspace or split the batch");
+  int dev = 0;
+  MSLR_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(MSLR_ERR_UNSUPPORTED, "device ordinal above 63");
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p)
+        return fail(MSLR_ERR_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch): ") +
+                                       cudaGetErrorString(e));
+      g_noalloc_addr[dev] = p;
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  // No part of the scratch has to start at zero: every stage writes what the
+  // next one reads, so the previous call's contents are simply overwritten.
+  return svst_batch(mrows, ncols, batch, betas, in, out, scratch, (size_t)MSLR_NOALLOC_SCRATCH_BYTES,
+                    st);
 }
 
 }  // namespace mslr
