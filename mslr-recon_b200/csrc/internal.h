@@ -62,6 +62,10 @@ struct Ctx {
   cf* d_T = nullptr;           // (F, Nc, nvox) per-coil k-space of a chunk of frames
   int F = 1;
   bool bound = false;
+  // tuned SENSE kernels (sense_fast.cu): plans and frames per chunk
+  bool fast = false;
+  alignas(16) unsigned char fplan_raw[3 * 256];   // fast::FPlan x, y, z (fft_fast.cuh)
+  int Ffast = 1;
 
   // POGM
   cf* d_U = nullptr;   // (Ns, Nt, nvox)
@@ -100,6 +104,13 @@ int sense_adjoint(Ctx* c, const cf* y, cf* x, cudaStream_t st);
 // g = A'(A Σ_k X_k − y) (subtract) or A'A Σ_k X_k
 int normal_op(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
               cudaStream_t st);
+
+// ---- sense_fast.cu (tuned form) ------------------------------------------------
+bool sense_fast_setup(Ctx* c);
+int normal_op_fast(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
+                   cudaStream_t st);
+int sense_forward_fast(Ctx* c, const cf* x, cf* y, cudaStream_t st);
+int sense_adjoint_fast(Ctx* c, const cf* y, cf* x, cudaStream_t st);
 
 // ---- svst.cu -----------------------------------------------------------------
 int svst_setup(Ctx* c);   // workspaces (create time)

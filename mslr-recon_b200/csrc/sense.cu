@@ -339,6 +339,11 @@ int sense_setup_tables(Ctx* c) {
   int rc = dalloc(c, (void**)&c->d_T, (size_t)c->F * c->Nc * c->nvox * sizeof(cf));
   if (rc) return rc;
   c->nwords = (int)((c->nvox + 31) / 32);
+  // tuned form: register-resident kernels when every axis has a fast plan;
+  // one frame per chunk so that the chunk's per-coil k-space can stay in L2
+  if (c->form == MSLR_FORM_TUNED)
+    c->fast = sense_fast_setup(c);
+  c->Ffast = 1;
   return MSLR_OK;
 }
 
@@ -374,6 +379,7 @@ int sense_bind(Ctx* c, const cf* smaps, const cf* y, const int32_t* idx, int bas
 }
 
 int sense_forward(Ctx* c, const cf* x, cf* y, cudaStream_t st) {
+  if (c->fast) return sense_forward_fast(c, x, y, st);
   const Dims d = dims_of(c);
   const float s = (float)(1.0 / std::sqrt((double)c->nvox));
   for (int t0 = 0; t0 < c->Nt; t0 += c->F) {
@@ -393,6 +399,7 @@ int sense_forward(Ctx* c, const cf* x, cf* y, cudaStream_t st) {
 }
 
 int sense_adjoint(Ctx* c, const cf* y, cf* x, cudaStream_t st) {
+  if (c->fast) return sense_adjoint_fast(c, y, x, st);
   const Dims d = dims_of(c);
   const float s = (float)(1.0 / std::sqrt((double)c->nvox));
   for (int t0 = 0; t0 < c->Nt; t0 += c->F) {
@@ -414,6 +421,7 @@ int sense_adjoint(Ctx* c, const cf* y, cf* x, cudaStream_t st) {
 
 int normal_op(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
               cudaStream_t st) {
+  if (c->fast) return normal_op_fast(c, X, ns, sstride, g, subtract, st);
   const Dims d = dims_of(c);
   const float scale = (float)(1.0 / (double)c->nvox);
   for (int t0 = 0; t0 < c->Nt; t0 += c->F) {

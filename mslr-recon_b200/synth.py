@@ -62,6 +62,11 @@ CONFIGS = {
     "precision": SynthConfig(N=(90, 90, 60), Nc=18, Nt=300, rank=8, frac=1 / 6, centre=12,
                              decay=1.5, patch_sizes=[[90, 90, 60], [10, 10, 10]],
                              strides=[[90, 90, 60], [10, 10, 10]], niters=50),
+    # the metric's image, coil and scale shapes with 8 frames: per-frame
+    # kernels are identical, so this is the case profiled with ncu
+    "profile": SynthConfig(N=(90, 90, 60), Nc=18, Nt=8, rank=8, frac=1 / 6, centre=12,
+                           patch_sizes=[[90, 90, 60], [10, 10, 10]],
+                           strides=[[90, 90, 60], [10, 10, 10]], niters=5),
     "diff": SynthConfig(N=(48, 48, 32), Nc=12, Nt=128, rank=8, frac=1 / 6, centre=8,
                         patch_sizes=[[48, 48, 32], [8, 8, 8]],
                         strides=[[48, 48, 32], [8, 8, 8]], niters=10),

@@ -9,6 +9,14 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+# The oracle runs many small LAPACK calls (one SVD per patch); a multithreaded
+# BLAS spends more time synchronising than computing on them.
+try:
+    from threadpoolctl import threadpool_limits
+    threadpool_limits(1, "blas")
+except Exception:
+    pass
+
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libmslr.so")

@@ -217,3 +217,30 @@ def test_state_errors(torch, M, gold):
     with M.MSLRContext((8, 6, 4), Nc, Nt, K, PATCHES[:1], STRIDES[:1]) as ctx:
         with pytest.raises(M.MSLRError, match="bind"):
             ctx.forward(dev(torch, gold["x"]))
+
+
+@pytest.mark.parametrize("form", ["plain", "tuned"])
+@pytest.mark.parametrize("N,Nc", [((90, 90, 60), 18), ((48, 48, 32), 12), ((45, 30, 20), 5),
+                                  ((32, 32, 24), 8), ((8, 6, 4), 3)])
+def test_sense_metric_shapes(torch, M, form, N, Nc):
+    """Forward, adjoint and normal operator at the benchmark image shapes
+    (two-pass radix plans in the tuned kernels; an odd axis included)."""
+    rng = np.random.default_rng(sum(N) + Nc)
+    Nx, Ny, Nz = N
+    Nt = 3
+    nvox = Nx * Ny * Nz
+    K = nvox // 6
+    smaps = (rng.standard_normal((Nc, Nz, Ny, Nx)) + 1j * rng.standard_normal((Nc, Nz, Ny, Nx)))
+    smaps /= np.sqrt(np.sum(np.abs(smaps) ** 2, axis=0))[None]
+    idx = np.stack([np.sort(rng.choice(nvox, K, replace=False)) for _ in range(Nt)]).astype(np.int32)
+    x = rng.standard_normal((Nt, Nz, Ny, Nx)) + 1j * rng.standard_normal((Nt, Nz, Ny, Nx))
+    y = rng.standard_normal((Nt, Nc, K)) + 1j * rng.standard_normal((Nt, Nc, K))
+    with M.MSLRContext(N, Nc, Nt, K, [[Nx, Ny, Nz]], [[Nx, Ny, Nz]], form=form) as ctx:
+        ctx.bind(dev(torch, smaps), dev(torch, y), dev(torch, idx, torch.int32))
+        yf = ctx.forward(dev(torch, x)).cpu().numpy()
+        assert rel(yf, O.sense_forward(x, smaps, idx)) < 1e-5
+        xa = ctx.adjoint(dev(torch, y)).cpu().numpy()
+        assert rel(xa, O.sense_adjoint(y, smaps, idx)) < 1e-5
+        g = ctx.normal(dev(torch, x[None])).cpu().numpy()
+        ref = O.sense_adjoint(O.sense_forward(x, smaps, idx) - y, smaps, idx)
+        assert rel(g, ref) < 1e-5
