@@ -1,0 +1,612 @@
+// eig.cu — per-patch Hermitian eigen stage of the patch SVST (sm_100a).
+//
+// For each patch Gram matrix G (n × n, Hermitian, column-major, FP32 complex)
+// and threshold β this computes the rebuild matrix
+//     W = V diag(h) Vᴴ,   h_i = max(√λ_i − β, 0) / √λ_i,
+// over the eigenpairs (λ_i, v_i) of G with λ_i > β² — the SVST of the patch
+// (src/recon.jl:183-211) expressed through its Gram matrix.  One CTA per
+// patch — 384 threads when n <= 384 (two patches per SM, so one patch's
+// latency-bound phases overlap the other's), else 1024; one launch may cover
+// several segments (the patches of several scales, each with its own n and
+// λ_k).  The matrix lives in global memory (L2):
+//   1. Householder tridiagonalisation G = Q T Qᴴ (FP32).  Each step applies
+//      the previous step's rank-2 update on the fly while forming the next
+//      matrix-vector product, so the trailing block is streamed once per step
+//      (thread i owns row i; column-major reads are coalesced).
+//   2. Eigenvalues of T above β² by bisection on FP64 Sturm counts, one
+//      thread per eigenvalue.
+//   3. Eigenvectors of T by FP64 twisted factorisation, one thread per
+//      eigenvector; eigenvalues equal to working precision (true
+//      degeneracies) are re-orthogonalised cooperatively by Gram–Schmidt.
+//   4. V = Q Z with the reflectors applied 16 at a time in compact WY form
+//      (Q_b = I − Y T Yᴴ); thread i keeps vector i's block coefficients in
+//      registers, so the update needs no cross-thread reduction.
+//   5. W = V diag(h) Vᴴ on 4×4 register tiles of the lower triangle,
+//      mirrored.
+// Zero patches give no eigenvalue above β² and W = 0 (the reference's
+// zero-norm skip, src/recon.jl:185).
+#include <cmath>
+
+#include "internal.h"
+
+namespace mslr {
+
+namespace {
+
+constexpr int kT = 1024;   // most threads per CTA (one row / eigenvalue per thread)
+constexpr int kSmallT = 384;   // CTA size for n <= 384: two patches share an SM
+constexpr int kNb = 16;    // reflectors per WY block
+constexpr int kVc = 16;    // eigenvectors per W staging chunk
+
+__device__ __forceinline__ float warp_sum(float v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block sums; every thread gets the result.  Consecutive calls must alternate
+// between two scratch buffers (one barrier per call).
+__device__ __forceinline__ float block_sum(float v, float* red) {
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float r = 0.f;
+  const int nw = (int)(blockDim.x >> 5);
+  for (int i = 0; i < nw; ++i) r += red[i];
+  return r;
+}
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+  v = warp_sum_d(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  const int nw = (int)(blockDim.x >> 5);
+  for (int i = 0; i < nw; ++i) r += red[i];
+  return r;
+}
+
+// eigenvalues of the symmetric tridiagonal (d, e²) strictly below x
+__device__ __forceinline__ int sturm_less(const double* d, const double* e2, int n, double x,
+                                          double pivmin) {
+  int cnt = 0;
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  cnt += (q < 0.0);
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += (q < 0.0);
+  }
+  return cnt;
+}
+
+struct Seg {
+  int n;
+  int64_t first;   // first block of the segment
+  int64_t np;      // patches
+  cf* gram;        // np × n × n: G in, Householder vectors, then W out
+  cf* zv;          // np × n × n: eigenvectors, [row j][vector i], i fastest
+  double* aux;     // np × n × n: FP64 pivots of the twisted factorisations
+  int* rank;       // np
+  double lam;      // threshold multiplier of the segment (λ_k)
+};
+
+constexpr int kMaxSeg = 8;
+
+struct EigArgs {
+  int nseg;
+  Seg seg[kMaxSeg];
+  const double* thr;   // device: threshold scale (ζ or β), or per patch
+  int thr_per_patch;
+};
+
+size_t smem_bytes(int n) {
+  const size_t vecs = 3 * (size_t)n * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
+                      3 * (size_t)n * sizeof(float) + 64 * sizeof(float) + 64 * sizeof(double);
+  const size_t wy = (size_t)n * kNb * sizeof(cf) + 2 * kNb * kNb * sizeof(cf);
+  const size_t wt = (size_t)n * kVc * sizeof(cf);
+  return vecs + std::max(wy, wt) + 128;
+}
+
+template <int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  int s = 0;
+  while (s + 1 < g.nseg && (int64_t)blockIdx.x >= g.seg[s + 1].first) ++s;
+  const Seg& S = g.seg[s];
+  const int n = S.n;
+  const int64_t ip = (int64_t)blockIdx.x - S.first;
+  const int tid = threadIdx.x;
+  const int kT = blockDim.x;   // n <= blockDim.x
+  cf* A = S.gram + ip * (int64_t)n * n;
+  cf* Z = S.zv + ip * (int64_t)n * n;
+  double* AUX = S.aux + ip * (int64_t)n * n;
+
+  // shared layout (8-byte aligned pieces first)
+  double* dd = reinterpret_cast<double*>(smraw);   // diagonal        [n]
+  double* ee = dd + n;                              // off-diagonal    [n]
+  double* ee2 = ee + n;                             // e²              [n]
+  double* lam = ee2 + n;                            // eigenvalues     [n]
+  double* redd = lam + n;                           // 64 doubles
+  cf* sv = reinterpret_cast<cf*>(redd + 64);        // v of this step  [n]
+  cf* svp = sv + n;                                 // previous v      [n]
+  cf* swp = svp + n;                                // previous w      [n]
+  float* hv = reinterpret_cast<float*>(swp + n);    // h               [n]
+  float* taur = hv + n;                             // τ               [n]
+  float* taui = taur + n;                           //                 [n]
+  float* red0 = taui + n;                           // 2 × 32 floats
+  float* red1 = red0 + 32;
+  cf* sY = reinterpret_cast<cf*>((reinterpret_cast<uintptr_t>(red1 + 32) + 15) & ~(uintptr_t)15);
+  __shared__ float s_bc[4];
+  __shared__ double s_bd[4];
+  __shared__ int s_r;
+
+  const double beta_d = g.thr[g.thr_per_patch ? (int64_t)blockIdx.x : 0] * S.lam;
+  const float beta = (float)beta_d;
+
+  // ---- 1. tridiagonalisation with delayed rank-2 updates ---------------------
+  for (int q = tid; q < n; q += kT) {
+    svp[q] = make_float2(0.f, 0.f);
+    swp[q] = make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const int i = tid;   // row owned by this thread (n <= kT)
+  for (int k = 0; k < n - 1; ++k) {
+    // current column k and diagonal k: stored − (vp wpᴴ + wp vpᴴ)
+    cf x = make_float2(0.f, 0.f);
+    cf vpi = make_float2(0.f, 0.f), wpi = make_float2(0.f, 0.f);
+    if (i < n) {
+      vpi = svp[i];
+      wpi = swp[i];
+    }
+    const cf vpk = svp[k], wpk = swp[k];
+    if (i >= k && i < n) {
+      x = A[(int64_t)k * n + i];
+      x = csub(x, cadd(cmul(vpi, cconj(wpk)), cmul(wpi, cconj(vpk))));
+      if (i == k) dd[k] = (double)x.x;
+    }
+    const float xn = block_sum((i >= k + 2 && i < n) ? cabs2(x) : 0.f, (k & 1) ? red1 : red0);
+    if (i == k + 1) {
+      // zlarfg: Hᴴ (α, x) = (β, 0), H = I − τ v vᴴ, β real
+      const float ar = x.x, ai = x.y;
+      float bt, tr, ti, sr, si;
+      if (xn == 0.f && ai == 0.f) {
+        bt = ar;
+        tr = ti = 0.f;
+        sr = 1.f;
+        si = 0.f;
+      } else {
+        bt = -copysignf(sqrtf(ar * ar + ai * ai + xn), ar);
+        tr = (bt - ar) / bt;
+        ti = -ai / bt;
+        const float zr = ar - bt, zi = ai;
+        const float den = zr * zr + zi * zi;
+        sr = zr / den;
+        si = -zi / den;
+      }
+      ee[k] = (double)bt;
+      ee2[k] = (double)bt * (double)bt;
+      taur[k] = tr;
+      taui[k] = ti;
+      s_bc[0] = tr;
+      s_bc[1] = ti;
+      s_bc[2] = sr;
+      s_bc[3] = si;
+    }
+    __syncthreads();
+    const cf tau = make_float2(s_bc[0], s_bc[1]);
+    const cf scal = make_float2(s_bc[2], s_bc[3]);
+    const bool refl = (tau.x != 0.f || tau.y != 0.f);
+    cf vi = make_float2(0.f, 0.f);
+    if (i == k + 1) {
+      vi = make_float2(1.f, 0.f);
+    } else if (i >= k + 2 && i < n) {
+      vi = cmul(x, scal);
+      A[(int64_t)k * n + i] = vi;   // reflector kept below the subdiagonal
+    }
+    if (i < n) sv[i] = vi;
+    __syncthreads();
+    // fused: A22 ← A22 − (vp wpᴴ + wp vpᴴ);  y = A22 v.  Loads are issued in
+    // batches of kB before the corresponding stores, so a thread keeps kB
+    // L2 requests in flight instead of one.
+    float yr = 0.f, yi = 0.f;
+    if (i >= k + 1 && i < n) {
+      constexpr int kB = 8;
+      cf* col = A + (int64_t)(k + 1) * n + i;
+      int j = k + 1;
+      for (; j + kB <= n; j += kB, col += (int64_t)kB * n) {
+        cf a[kB];
+#pragma unroll
+        for (int b = 0; b < kB; ++b) a[b] = __ldcg(col + (int64_t)b * n);
+#pragma unroll
+        for (int b = 0; b < kB; ++b) {
+          const cf vpj = svp[j + b], wpj = swp[j + b], vj = sv[j + b];
+          a[b].x -= (vpi.x * wpj.x + vpi.y * wpj.y) + (wpi.x * vpj.x + wpi.y * vpj.y);
+          a[b].y -= (vpi.y * wpj.x - vpi.x * wpj.y) + (wpi.y * vpj.x - wpi.x * vpj.y);
+          yr += a[b].x * vj.x - a[b].y * vj.y;
+          yi += a[b].x * vj.y + a[b].y * vj.x;
+        }
+#pragma unroll
+        for (int b = 0; b < kB; ++b) col[(int64_t)b * n] = a[b];
+      }
+      for (; j < n; ++j, col += n) {
+        cf a = __ldcg(col);
+        const cf vpj = svp[j], wpj = swp[j], vj = sv[j];
+        a.x -= (vpi.x * wpj.x + vpi.y * wpj.y) + (wpi.x * vpj.x + wpi.y * vpj.y);
+        a.y -= (vpi.y * wpj.x - vpi.x * wpj.y) + (wpi.y * vpj.x - wpi.x * vpj.y);
+        *col = a;
+        yr += a.x * vj.x - a.y * vj.y;
+        yi += a.x * vj.y + a.y * vj.x;
+      }
+    }
+    // vᴴ y (real for Hermitian A)
+    const float vy = block_sum((i >= k + 1 && i < n) ? (vi.x * yr + vi.y * yi) : 0.f,
+                               (k & 1) ? red0 : red1);
+    const float c = 0.5f * (tau.x * tau.x + tau.y * tau.y) * vy;
+    if (i < n) {
+      cf w = make_float2(0.f, 0.f);
+      if (i >= k + 1 && refl) {
+        const cf ty = cmul(tau, make_float2(yr, yi));
+        w = make_float2(ty.x - c * vi.x, ty.y - c * vi.y);
+      }
+      swp[i] = w;
+      svp[i] = refl ? vi : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+  }
+  if (i == n - 1) {
+    cf x = A[(int64_t)(n - 1) * n + (n - 1)];
+    const cf vpk = svp[n - 1], wpk = swp[n - 1];
+    x = csub(x, cadd(cmul(vpk, cconj(wpk)), cmul(wpk, cconj(vpk))));
+    dd[n - 1] = (double)x.x;
+    ee[n - 1] = 0.0;
+    ee2[n - 1] = 0.0;
+  }
+  __syncthreads();
+
+  // ---- 2. eigenvalues above β² (FP64 bisection, thread per eigenvalue) -------
+  if (tid == 0) {
+    double gl = dd[0], gu = dd[0], emax2 = 0.0;
+    for (int q = 0; q < n; ++q) {
+      const double rr = (q > 0 ? fabs(ee[q - 1]) : 0.0) + (q < n - 1 ? fabs(ee[q]) : 0.0);
+      gl = fmin(gl, dd[q] - rr);
+      gu = fmax(gu, dd[q] + rr);
+      if (q < n - 1) emax2 = fmax(emax2, ee2[q]);
+    }
+    const double tnorm = fmax(fabs(gl), fabs(gu));
+    const double pivmin = fmax(2.2250738585072014e-308 * fmax(emax2, 1.0), 1e-290);
+    const double pad = 2.0 * 2.220446049250313e-16 * tnorm * n + pivmin;
+    gl -= pad;
+    gu += pad;
+    s_bd[0] = gl;
+    s_bd[1] = gu;
+    s_bd[2] = pivmin;
+    s_bd[3] = tnorm;
+    const double thr2 = beta_d * beta_d;
+    s_r = (thr2 >= gu) ? 0 : n - sturm_less(dd, ee2, n, thr2, pivmin);
+  }
+  __syncthreads();
+  const int r = s_r;
+  const double gl = fmax(s_bd[0], beta_d * beta_d), gu = s_bd[1], pivmin = s_bd[2],
+               tnorm = s_bd[3];
+  if (tid == 0) S.rank[ip] = r;
+  if (tid < r) {
+    const int kth = n - 1 - tid;   // tid-th largest = kth smallest
+    double lo = gl, hi = gu;
+    for (int it = 0; it < 80; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (mid <= lo || mid >= hi) break;
+      if (sturm_less(dd, ee2, n, mid, pivmin) > kth) hi = mid;
+      else lo = mid;
+    }
+    const double lm = 0.5 * (lo + hi);
+    lam[tid] = lm;
+    const double sg = sqrt(fmax(lm, 0.0));
+    hv[tid] = (sg > beta_d && sg > 0.0) ? (float)((sg - beta_d) / sg) : 0.f;
+  }
+  __syncthreads();
+  if (r == 0) {
+    for (int64_t q = tid; q < (int64_t)n * n; q += kT) A[q] = make_float2(0.f, 0.f);
+    return;
+  }
+
+  // ---- 3. eigenvectors of T (FP64 twisted factorisation) --------------------
+  // D+ in AUX[j][i]; D− and then z_j in the Z slot [j][i] read as a double;
+  // finally converted in place to complex float.
+  if (tid < r) {
+    const double lm = lam[tid];
+    double* dp = AUX + tid;
+    double* zd = reinterpret_cast<double*>(Z) + tid;
+    double q = dd[0] - lm;
+    if (fabs(q) < pivmin) q = -pivmin;
+    dp[0] = q;
+    for (int j = 0; j + 1 < n; ++j) {
+      q = dd[j + 1] - lm - ee2[j] / q;
+      if (fabs(q) < pivmin) q = -pivmin;
+      dp[(int64_t)(j + 1) * n] = q;
+    }
+    q = dd[n - 1] - lm;
+    if (fabs(q) < pivmin) q = -pivmin;
+    zd[(int64_t)(n - 1) * n] = q;
+    int kb = n - 1;
+    double gb = fabs(dp[(int64_t)(n - 1) * n] + q - (dd[n - 1] - lm));
+    for (int j = n - 2; j >= 0; --j) {
+      q = dd[j] - lm - ee2[j] / q;
+      if (fabs(q) < pivmin) q = -pivmin;
+      zd[(int64_t)j * n] = q;
+      const double gm = fabs(dp[(int64_t)j * n] + q - (dd[j] - lm));
+      if (gm < gb) {
+        gb = gm;
+        kb = j;
+      }
+    }
+    double nrm = 1.0, zp = 1.0;
+    for (int j = kb - 1; j >= 0; --j) {   // z_j = −e_j z_{j+1} / D+_j
+      zp = -ee[j] * zp / dp[(int64_t)j * n];
+      zd[(int64_t)j * n] = zp;
+      nrm += zp * zp;
+    }
+    zd[(int64_t)kb * n] = 1.0;
+    zp = 1.0;
+    for (int j = kb + 1; j < n; ++j) {    // z_j = −e_{j−1} z_{j−1} / D−_j
+      zp = -ee[j - 1] * zp / zd[(int64_t)j * n];
+      zd[(int64_t)j * n] = zp;
+      nrm += zp * zp;
+    }
+    const double inv = 1.0 / sqrt(nrm);
+    cf* zc = Z + tid;
+    for (int j = 0; j < n; ++j) {
+      const double zj = zd[(int64_t)j * n];
+      zc[(int64_t)j * n] = make_float2((float)(zj * inv), 0.f);
+    }
+  }
+  __syncthreads();
+  // Eigenvalues equal to working precision: Gram–Schmidt inside the cluster,
+  // cooperatively (every thread walks the same clusters).
+  {
+    const double ctol = 1e-12 * fmax(tnorm, 1e-300);
+    int s0 = 0;
+    int rb = 0;
+    while (s0 < r) {
+      int t = s0 + 1;
+      while (t < r && lam[t - 1] - lam[t] <= ctol) ++t;
+      for (int qv = s0 + 1; qv < t; ++qv) {
+        for (int attempt = 0; attempt < 4; ++attempt) {
+          for (int pv = s0; pv < qv; ++pv) {
+            double dot = 0.0;
+            for (int j = tid; j < n; j += kT) dot += (double)Z[(int64_t)j * n + pv].x * Z[(int64_t)j * n + qv].x;
+            dot = block_sum_d(dot, redd + 32 * (rb++ & 1));
+            for (int j = tid; j < n; j += kT) Z[(int64_t)j * n + qv].x -= (float)dot * Z[(int64_t)j * n + pv].x;
+            __syncthreads();
+          }
+          double nr = 0.0;
+          for (int j = tid; j < n; j += kT) nr += (double)Z[(int64_t)j * n + qv].x * Z[(int64_t)j * n + qv].x;
+          nr = sqrt(block_sum_d(nr, redd + 32 * (rb++ & 1)));
+          if (nr > 0.1) {
+            for (int j = tid; j < n; j += kT) Z[(int64_t)j * n + qv].x /= (float)nr;
+            __syncthreads();
+            break;
+          }
+          // collapsed onto earlier vectors: restart from a unit vector
+          for (int j = tid; j < n; j += kT)
+            Z[(int64_t)j * n + qv].x = (j == (qv + attempt * 7919) % n) ? 1.f : 0.f;
+          __syncthreads();
+        }
+      }
+      s0 = t;
+    }
+  }
+
+  // ---- 4. V = H_0 ⋯ H_{n-2} Z, blocks of kNb reflectors from the last ---------
+  cf* sT = sY + (int64_t)n * kNb;   // kNb × kNb, T[a][b] at a*kNb + b
+  cf* sYY = sT + kNb * kNb;         // Yᴴ Y
+  const int nref = n - 1;
+  for (int kend = nref; kend > 0; kend -= kNb) {
+    const int k0 = max(0, kend - kNb);
+    const int nb = kend - k0;
+    for (int q = tid; q < n * kNb; q += kT) {   // Y: column jj = reflector k0 + jj
+      const int row = q / kNb, jj = q - row * kNb;
+      const int k = k0 + jj;
+      cf y = make_float2(0.f, 0.f);
+      if (jj < nb) {
+        if (row == k + 1) y = make_float2(1.f, 0.f);
+        else if (row > k + 1) y = A[(int64_t)k * n + row];
+      }
+      sY[q] = y;
+    }
+    __syncthreads();
+    if (tid < kNb * kNb) {   // Yᴴ Y
+      const int a = tid / kNb, b = tid - a * kNb;
+      float sr = 0.f, si = 0.f;
+      for (int row = k0 + 1; row < n; ++row) {
+        const cf ya = sY[row * kNb + a], yb = sY[row * kNb + b];
+        sr += ya.x * yb.x + ya.y * yb.y;
+        si += ya.x * yb.y - ya.y * yb.x;
+      }
+      sYY[tid] = make_float2(sr, si);
+    }
+    __syncthreads();
+    if (tid < 32) {   // zlarft (forward, columnwise); lane a owns row a of T
+      const int a = tid;
+      for (int jj = 0; jj < kNb; ++jj) {
+        const cf tj = (jj < nb) ? make_float2(taur[k0 + jj], taui[k0 + jj]) : make_float2(0.f, 0.f);
+        if (a < jj) {
+          cf sacc = make_float2(0.f, 0.f);
+          for (int b = a; b < jj; ++b) sacc = cadd(sacc, cmul(sT[a * kNb + b], sYY[b * kNb + jj]));
+          const cf v = cmul(tj, sacc);
+          sT[a * kNb + jj] = make_float2(-v.x, -v.y);
+        } else if (a < kNb) {
+          sT[a * kNb + jj] = (a == jj) ? tj : make_float2(0.f, 0.f);
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    if (tid < r) {   // vector tid: S = Yᴴ z;  S ← T S;  z −= Y S
+      cf Sv[kNb];
+#pragma unroll
+      for (int jj = 0; jj < kNb; ++jj) Sv[jj] = make_float2(0.f, 0.f);
+      for (int row = k0 + 1; row < n; ++row) {
+        const cf z = Z[(int64_t)row * n + tid];
+#pragma unroll
+        for (int jj = 0; jj < kNb; ++jj) {
+          const cf y = sY[row * kNb + jj];   // conj(y)·z
+          Sv[jj].x += y.x * z.x + y.y * z.y;
+          Sv[jj].y += y.x * z.y - y.y * z.x;
+        }
+      }
+      // T upper-triangular: S[a] is last needed by row a itself (in place)
+#pragma unroll
+      for (int a = 0; a < kNb; ++a) {
+        cf sacc = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int b = a; b < kNb; ++b) sacc = cadd(sacc, cmul(sT[a * kNb + b], Sv[b]));
+        Sv[a] = sacc;
+      }
+      constexpr int kB = 8;   // rows per batch: loads issued before stores
+      int row = k0 + 1;
+      for (; row + kB <= n; row += kB) {
+        cf z[kB];
+#pragma unroll
+        for (int b = 0; b < kB; ++b) z[b] = __ldcg(Z + (int64_t)(row + b) * n + tid);
+#pragma unroll
+        for (int b = 0; b < kB; ++b) {
+#pragma unroll
+          for (int jj = 0; jj < kNb; ++jj) z[b] = csub(z[b], cmul(sY[(row + b) * kNb + jj], Sv[jj]));
+        }
+#pragma unroll
+        for (int b = 0; b < kB; ++b) Z[(int64_t)(row + b) * n + tid] = z[b];
+      }
+      for (; row < n; ++row) {
+        cf z = Z[(int64_t)row * n + tid];
+#pragma unroll
+        for (int jj = 0; jj < kNb; ++jj) z = csub(z, cmul(sY[row * kNb + jj], Sv[jj]));
+        Z[(int64_t)row * n + tid] = z;
+      }
+    }
+    __syncthreads();
+  }
+
+  // ---- 5. W = V diag(h) Vᴴ, lower 4×4 tiles, mirrored into A ------------------
+  cf* sVc = sY;   // staging: sVc[row*kVc + c] = √h_c · V[row][i0 + c]
+  const int nt4 = (n + 3) / 4;
+  const int ntiles = nt4 * (nt4 + 1) / 2;
+  for (int tile0 = 0; tile0 < ntiles; tile0 += kT) {
+    const int tile = tile0 + tid;
+    int ta = 0, tb = 0;
+    const bool act = tile < ntiles;
+    if (act) {
+      ta = (int)((sqrtf(8.f * tile + 1.f) - 1.f) * 0.5f);
+      while ((ta + 1) * (ta + 2) / 2 <= tile) ++ta;
+      while (ta * (ta + 1) / 2 > tile) --ta;
+      tb = tile - ta * (ta + 1) / 2;
+    }
+    cf acc[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[p][q] = make_float2(0.f, 0.f);
+    for (int i0 = 0; i0 < r; i0 += kVc) {
+      const int cnt = min(kVc, r - i0);
+      __syncthreads();
+      for (int q = tid; q < n * kVc; q += kT) {
+        const int row = q / kVc, c = q - row * kVc;
+        sVc[q] = (c < cnt) ? cscale(Z[(int64_t)row * n + i0 + c], sqrtf(hv[i0 + c]))
+                           : make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+      if (act) {
+        for (int c = 0; c < cnt; ++c) {
+          cf va[4], vb[4];
+#pragma unroll
+          for (int p = 0; p < 4; ++p) {
+            const int a = ta * 4 + p, b = tb * 4 + p;
+            va[p] = (a < n) ? sVc[a * kVc + c] : make_float2(0.f, 0.f);
+            vb[p] = (b < n) ? sVc[b * kVc + c] : make_float2(0.f, 0.f);
+          }
+#pragma unroll
+          for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {   // va · conj(vb)
+              acc[p][q].x += va[p].x * vb[q].x + va[p].y * vb[q].y;
+              acc[p][q].y += va[p].y * vb[q].x - va[p].x * vb[q].y;
+            }
+        }
+      }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int a = ta * 4 + p, b = tb * 4 + q;
+          if (a < n && b < n) {
+            A[(int64_t)b * n + a] = acc[p][q];
+            A[(int64_t)a * n + b] = cconj(acc[p][q]);
+          }
+        }
+    }
+  }
+}
+
+}  // namespace
+
+int eig2_prepare(int nmax) {
+  if (nmax > kT) return fail(MSLR_ERR_UNSUPPORTED, "Gram side above 1024");
+  const size_t sm = smem_bytes(nmax);
+  if (sm > 227 * 1024) return fail(MSLR_ERR_UNSUPPORTED, "Gram side too large for the eigen stage");
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  if (nmax <= kSmallT)
+    MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm));
+  return MSLR_OK;
+}
+
+int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int thr_per_patch,
+                     cudaStream_t st) {
+  if (nseg < 1 || nseg > kMaxSeg) return fail(MSLR_ERR_UNSUPPORTED, "too many scales in one launch");
+  EigArgs a;
+  a.nseg = nseg;
+  a.thr = thr;
+  a.thr_per_patch = thr_per_patch;
+  int64_t total = 0;
+  int nmax = 1;
+  for (int s = 0; s < nseg; ++s) {
+    Seg& S = a.seg[s];
+    S.n = segs[s].n;
+    S.first = total;
+    S.np = segs[s].np;
+    S.gram = segs[s].gram;
+    S.zv = segs[s].zv;
+    S.aux = segs[s].aux;
+    S.rank = segs[s].rank;
+    S.lam = segs[s].lam;
+    total += segs[s].np;
+    nmax = std::max(nmax, segs[s].n);
+  }
+  if (nmax <= kSmallT)
+    k_eig<kSmallT, 2><<<(unsigned)total, kSmallT, smem_bytes(nmax), st>>>(a);
+  else
+    k_eig<kT, 1><<<(unsigned)total, kT, smem_bytes(nmax), st>>>(a);
+  MSLR_CUDA_TRY(cudaGetLastError());
+  return MSLR_OK;
+}
+
+int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, const double* thr,
+                int thr_per_patch, double lam, cudaStream_t st) {
+  EigSegment s;
+  s.n = n;
+  s.np = np;
+  s.gram = gram;
+  s.zv = zv;
+  s.aux = reinterpret_cast<double*>(aux);
+  s.rank = rank;
+  s.lam = lam;
+  return eig_launch_multi(1, &s, thr, thr_per_patch, st);
+}
+
+}  // namespace mslr

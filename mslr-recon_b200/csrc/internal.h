@@ -115,11 +115,29 @@ int sense_adjoint_fast(Ctx* c, const cf* y, cf* x, cudaStream_t st);
 // ---- svst.cu -----------------------------------------------------------------
 int svst_setup(Ctx* c);   // workspaces (create time)
 // img_out = patchSVST(img_in) for scale s with threshold (*thr_dev) * lam
+int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaStream_t st);
 int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_in, cf* img_out,
                cudaStream_t st);
 int geom_build(const int N[3], int Nt, const int ps_in[3], const int ss_in[3], ScaleGeom* g);
 int geom_upload(ScaleGeom* g, const int N[3]);
 void geom_free(ScaleGeom* g);
+
+// ---- eig.cu --------------------------------------------------------------------
+// One group of patches that share a Gram side n and a threshold multiplier.
+struct EigSegment {
+  int n;
+  int64_t np;
+  cf* gram;      // np × n × n: Gram in, W out
+  cf* zv;        // np × n × n scratch
+  double* aux;   // np × n × n scratch
+  int* rank;     // np
+  double lam;
+};
+int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int thr_per_patch,
+                     cudaStream_t st);
+int eig2_prepare(int nmax);
+int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, const double* thr,
+                int thr_per_patch, double lam, cudaStream_t st);
 
 // ---- pogm.cu -----------------------------------------------------------------
 int pogm_setup(Ctx* c);

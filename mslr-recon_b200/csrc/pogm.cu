@@ -250,7 +250,9 @@ int pogm_step(Ctx* c, cf* X, cudaStream_t st) {
                                            c->d_restarts, c->d_err);
   MSLR_CUDA_TRY(cudaGetLastError());
   c->launches += 3;
-  // 4. x_i = g_prox(z_i, ζ): per-scale patch SVST with threshold ζ·λ_k
+  // 4. x_i = g_prox(z_i, ζ): patch SVST with threshold ζ·λ_k — scale after
+  //    scale in the plain form, all scales batched in the tuned form
+  if (c->form == MSLR_FORM_TUNED) return patch_svst_all(c, c->d_thr, c->d_Z, X, st);
   for (int k = 0; k < c->Ns; ++k) {
     if ((rc = patch_svst(c, k, c->d_thr, c->lambdas[k], c->d_Z + k * E, X + k * E, st)))
       return rc;

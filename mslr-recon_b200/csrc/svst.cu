@@ -14,11 +14,7 @@
 // skip (src/recon.jl:185) falls out without a special case.
 //
 // Per patch (one CTA):
-//   1. Householder tridiagonalisation of G (FP32, FP64 reductions),
-//   2. eigenvalues above β² by Sturm bisection on the real tridiagonal (FP64),
-//   3. eigenvectors by twisted factorisation (FP64), MGS within tight clusters,
-//   4. back-transformation by the Householder reflectors,
-//   5. W = V diag(h) Vᴴ.
+//   Gram (this file) → eigen stage producing W (eig.cu) → rebuild (this file).
 // Patches never see a host loop: every stage is one launch over all patches
 // of a scale.  Overlapping or gapped patch grids are recombined by a gather
 // over covering patches in ascending ip order with the Float32 coverage
@@ -33,7 +29,6 @@ namespace mslr {
 
 namespace {
 
-constexpr int kEigThreads = 256;
 constexpr int kTile = 64;
 constexpr int kKc = 16;
 
@@ -171,353 +166,6 @@ __global__ void k_gram_reduce(const cf* __restrict__ part, cf* __restrict__ G, i
     cf s = part[e];
     for (int q = 1; q < nsplit; ++q) s = cadd(s, part[q * nn + e]);
     G[e] = s;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Per-patch eigen stage.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_sum_d(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// block-wide double sum; result broadcast to all threads
-__device__ double block_sum_all(double v, double* sh) {
-  v = warp_sum_d(v);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) sh[w] = v;
-  __syncthreads();
-  double r = 0.0;
-  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) r += sh[i];
-  return r;
-}
-
-// number of eigenvalues of the symmetric tridiagonal (d, e) strictly below x
-__device__ int sturm_less(const double* d, const double* e, int n, double x, double pivmin) {
-  int cnt = 0;
-  double q = d[0] - x;
-  if (fabs(q) < pivmin) q = -pivmin;
-  if (q < 0) ++cnt;
-  for (int i = 1; i < n; ++i) {
-    q = d[i] - x - (e[i - 1] * e[i - 1]) / q;
-    if (fabs(q) < pivmin) q = -pivmin;
-    if (q < 0) ++cnt;
-  }
-  return cnt;
-}
-
-struct EigArgs {
-  int n;
-  cf* gram;          // np*n*n
-  void* zv;          // np*n*n × 8 bytes
-  double* aux;       // np*n*n
-  double* vecs;      // np*6*n
-  int* rank;         // np
-  const double* thr; // device threshold(s)
-  int thr_per_patch;
-  double lam;
-};
-
-__global__ void __launch_bounds__(kEigThreads) k_eig(EigArgs g) {
-  extern __shared__ unsigned char smraw[];
-  const int n = g.n;
-  const int64_t ip = blockIdx.x;
-  cf* A = g.gram + ip * (int64_t)n * n;
-  double* Z = reinterpret_cast<double*>(g.zv) + ip * (int64_t)n * n;
-  cf* V = reinterpret_cast<cf*>(g.zv) + ip * (int64_t)n * n;
-  double* AUX = g.aux + ip * (int64_t)n * n;
-  double* vec = g.vecs + ip * (int64_t)6 * n;
-  double* d = vec;              // n
-  double* e = vec + n;          // n
-  double* taur = vec + 2 * n;   // n
-  double* taui = vec + 3 * n;   // n
-  double* lamv = vec + 4 * n;   // n
-  double* hv = vec + 5 * n;     // n
-  cf* sv = reinterpret_cast<cf*>(smraw);   // n
-  cf* sy = sv + n;                          // n (y then w)
-  double* red = reinterpret_cast<double*>(sy + n);  // 32
-  __shared__ double s_bc[8];
-  __shared__ int s_r;
-  const int tid = threadIdx.x, nt = blockDim.x;
-
-  const double beta = g.thr[g.thr_per_patch ? ip : 0] * g.lam;
-  const double thr2 = beta * beta;
-
-  // ---- 1. Householder tridiagonalisation, A ← Hᴴ A H per step --------------
-  for (int k = 0; k < n - 1; ++k) {
-    const int m = n - k - 1;
-    cf* colk = A + (int64_t)k * n;
-    double xn = 0.0;
-    for (int i = k + 2 + tid; i < n; i += nt) {
-      const cf v = colk[i];
-      xn += (double)v.x * v.x + (double)v.y * v.y;
-    }
-    xn = block_sum_all(xn, red);
-    if (tid == 0) {
-      const cf al = colk[k + 1];
-      const double ar = al.x, ai = al.y;
-      double bt, tr, ti, sr, si;
-      if (xn == 0.0 && ai == 0.0) {
-        bt = ar;
-        tr = ti = 0.0;
-        sr = 1.0;
-        si = 0.0;
-      } else {
-        bt = -copysign(sqrt(ar * ar + ai * ai + xn), ar);
-        tr = (bt - ar) / bt;
-        ti = -ai / bt;
-        const double zr = ar - bt, zi = ai;
-        const double den = zr * zr + zi * zi;
-        sr = zr / den;
-        si = -zi / den;
-      }
-      d[k] = (double)colk[k].x;
-      e[k] = bt;
-      taur[k] = tr;
-      taui[k] = ti;
-      s_bc[0] = tr;
-      s_bc[1] = ti;
-      s_bc[2] = sr;
-      s_bc[3] = si;
-    }
-    __syncthreads();
-    const float tr = (float)s_bc[0], ti = (float)s_bc[1];
-    const cf scal = make_float2((float)s_bc[2], (float)s_bc[3]);
-    for (int i = tid; i < m; i += nt) {
-      cf v;
-      if (i == 0) {
-        v = make_float2(1.f, 0.f);
-      } else {
-        v = cmul(colk[k + 1 + i], scal);
-        colk[k + 1 + i] = v;   // Householder vector kept below the subdiagonal
-      }
-      sv[i] = v;
-    }
-    __syncthreads();
-    if (tr == 0.f && ti == 0.f) continue;
-    const cf tau = make_float2(tr, ti);
-    // y = A22 v
-    cf* A22 = A + (int64_t)(k + 1) * n + (k + 1);
-    for (int i = tid; i < m; i += nt) {
-      float yr = 0.f, yi = 0.f;
-      for (int j = 0; j < m; ++j) {
-        const cf a = A22[(int64_t)j * n + i];
-        const cf v = sv[j];
-        yr += a.x * v.x - a.y * v.y;
-        yi += a.x * v.y + a.y * v.x;
-      }
-      sy[i] = make_float2(yr, yi);
-    }
-    __syncthreads();
-    double vy = 0.0;   // Re(vᴴ y)
-    for (int i = tid; i < m; i += nt) vy += (double)sv[i].x * sy[i].x + (double)sv[i].y * sy[i].y;
-    vy = block_sum_all(vy, red);
-    const float cst = (float)(0.5 * ((double)tr * tr + (double)ti * ti) * vy);
-    for (int i = tid; i < m; i += nt) {
-      const cf w = csub(cmul(tau, sy[i]), cscale(sv[i], cst));
-      sy[i] = w;
-    }
-    __syncthreads();
-    // A22 −= w vᴴ + v wᴴ
-    for (int i = tid; i < m; i += nt) {
-      const cf wi = sy[i], vi = sv[i];
-      for (int j = 0; j < m; ++j) {
-        const cf vj = sv[j], wj = sy[j];
-        cf a = A22[(int64_t)j * n + i];
-        a = csub(a, cmul(wi, cconj(vj)));
-        a = csub(a, cmul(vi, cconj(wj)));
-        A22[(int64_t)j * n + i] = a;
-      }
-    }
-    __syncthreads();
-  }
-  if (tid == 0) {
-    d[n - 1] = (double)A[(int64_t)(n - 1) * n + (n - 1)].x;
-    if (n >= 1) e[n - 1] = 0.0;
-  }
-  __syncthreads();
-
-  // ---- 2. eigenvalues above β² --------------------------------------------
-  if (tid == 0) {
-    double gl = d[0], gu = d[0], emax2 = 0.0;
-    for (int i = 0; i < n; ++i) {
-      const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0);
-      gl = fmin(gl, d[i] - r);
-      gu = fmax(gu, d[i] + r);
-      if (i < n - 1) emax2 = fmax(emax2, e[i] * e[i]);
-    }
-    const double tnorm = fmax(fabs(gl), fabs(gu));
-    const double pivmin = fmax(2.2250738585072014e-308 * fmax(emax2, 1.0), 1e-300);
-    gl -= 2.0 * 2.220446049250313e-16 * tnorm * n + pivmin;
-    gu += 2.0 * 2.220446049250313e-16 * tnorm * n + pivmin;
-    s_bc[4] = gl;
-    s_bc[5] = gu;
-    s_bc[6] = pivmin;
-    s_bc[7] = tnorm;
-    const int below = sturm_less(d, e, n, thr2, pivmin);
-    s_r = (thr2 >= gu) ? 0 : n - below;
-  }
-  __syncthreads();
-  const int r = s_r;
-  const double gl = s_bc[4], gu = s_bc[5], pivmin = s_bc[6], tnorm = s_bc[7];
-  if (tid == 0) g.rank[ip] = r;
-  for (int i = tid; i < r; i += nt) {
-    const int kth = n - 1 - i;   // kth smallest
-    double lo = gl, hi = gu;
-    for (int it = 0; it < 200; ++it) {
-      const double mid = 0.5 * (lo + hi);
-      if (hi - lo <= 2.220446049250313e-16 * fmax(fabs(lo), fabs(hi)) + pivmin || mid == lo ||
-          mid == hi)
-        break;
-      if (sturm_less(d, e, n, mid, pivmin) > kth) hi = mid;
-      else lo = mid;
-    }
-    const double lm = 0.5 * (lo + hi);
-    lamv[i] = lm;
-    const double sg = sqrt(fmax(lm, 0.0));
-    hv[i] = (sg > beta && sg > 0.0) ? (sg - beta) / sg : 0.0;
-  }
-  __syncthreads();
-  if (r == 0) {
-    for (int64_t q = tid; q < (int64_t)n * n; q += nt) A[q] = make_float2(0.f, 0.f);
-    return;
-  }
-
-  // ---- 3. eigenvectors of T by twisted factorisation -------------------------
-  for (int i = tid; i < r; i += nt) {
-    const double lm = lamv[i];
-    double* z = Z + (int64_t)i * n;     // holds D+ then z
-    double* dm = AUX + (int64_t)i * n;  // D−
-    z[0] = d[0] - lm;
-    if (fabs(z[0]) < pivmin) z[0] = -pivmin;
-    for (int j = 0; j + 1 < n; ++j) {
-      double q = d[j + 1] - lm - e[j] * e[j] / z[j];
-      if (fabs(q) < pivmin) q = -pivmin;
-      z[j + 1] = q;
-    }
-    dm[n - 1] = d[n - 1] - lm;
-    if (fabs(dm[n - 1]) < pivmin) dm[n - 1] = -pivmin;
-    for (int j = n - 2; j >= 0; --j) {
-      double q = d[j] - lm - e[j] * e[j] / dm[j + 1];
-      if (fabs(q) < pivmin) q = -pivmin;
-      dm[j] = q;
-    }
-    int kb = 0;
-    double gb = INFINITY;
-    for (int j = 0; j < n; ++j) {
-      const double gm = fabs(z[j] + dm[j] - (d[j] - lm));
-      if (gm < gb) {
-        gb = gm;
-        kb = j;
-      }
-    }
-    // z_kb = 1; upward with D+, downward with D−
-    double nrm = 1.0;
-    double zprev = 1.0;
-    for (int j = kb - 1; j >= 0; --j) {
-      const double zj = -e[j] * zprev / z[j];
-      z[j] = zj;
-      zprev = zj;
-      nrm += zj * zj;
-    }
-    z[kb] = 1.0;
-    zprev = 1.0;
-    for (int j = kb + 1; j < n; ++j) {
-      const double zj = -e[j - 1] * zprev / dm[j];
-      z[j] = zj;
-      zprev = zj;
-      nrm += zj * zj;
-    }
-    const double inv = 1.0 / sqrt(nrm);
-    for (int j = 0; j < n; ++j) z[j] *= inv;
-  }
-  __syncthreads();
-  // tight clusters: modified Gram–Schmidt (one thread; clusters are rare)
-  if (tid == 0) {
-    const double ctol = 1e-10 * fmax(tnorm, 1e-300);
-    int s = 0;
-    while (s < r) {
-      int t = s + 1;
-      while (t < r && lamv[t - 1] - lamv[t] <= ctol) ++t;
-      if (t - s > 1) {
-        for (int q = s; q < t; ++q) {
-          double* zq = Z + (int64_t)q * n;
-          for (int attempt = 0; attempt < 4; ++attempt) {
-            for (int p2 = s; p2 < q; ++p2) {
-              const double* zp = Z + (int64_t)p2 * n;
-              double dot = 0.0;
-              for (int j = 0; j < n; ++j) dot += zp[j] * zq[j];
-              for (int j = 0; j < n; ++j) zq[j] -= dot * zp[j];
-            }
-            double nr = 0.0;
-            for (int j = 0; j < n; ++j) nr += zq[j] * zq[j];
-            nr = sqrt(nr);
-            if (nr > 0.1) {
-              for (int j = 0; j < n; ++j) zq[j] /= nr;
-              break;
-            }
-            // collapsed: restart from a deterministic unit vector and retry
-            for (int j = 0; j < n; ++j) zq[j] = 0.0;
-            zq[(q + attempt * 7919) % n] = 1.0;
-          }
-        }
-      }
-      s = t;
-    }
-  }
-  __syncthreads();
-
-  // ---- 4. back-transformation V = H_0 … H_{n-2} Z ----------------------------
-  for (int i = tid; i < r; i += nt) {
-    double* z = Z + (int64_t)i * n;
-    cf* vcol = V + (int64_t)i * n;
-    for (int j = 0; j < n; ++j) {
-      const double zj = z[j];
-      vcol[j] = make_float2((float)zj, 0.f);
-    }
-  }
-  __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-  for (int k = n - 2; k >= 0; --k) {
-    const float tr = (float)taur[k], ti = (float)taui[k];
-    if (tr == 0.f && ti == 0.f) continue;
-    const int m = n - k - 1;
-    const cf* colk = A + (int64_t)k * n;
-    for (int i = tid; i < m; i += nt) sv[i] = (i == 0) ? make_float2(1.f, 0.f) : colk[k + 1 + i];
-    __syncthreads();
-    const cf tau = make_float2(tr, ti);
-    for (int j = warp; j < r; j += nw) {
-      cf* vc = V + (int64_t)j * n + (k + 1);
-      float sr = 0.f, si = 0.f;
-      for (int i = lane; i < m; i += 32) {
-        const cf a = sv[i], b = vc[i];   // conj(a)·b
-        sr += a.x * b.x + a.y * b.y;
-        si += a.x * b.y - a.y * b.x;
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        sr += __shfl_xor_sync(0xffffffffu, sr, o);
-        si += __shfl_xor_sync(0xffffffffu, si, o);
-      }
-      const cf ts = cmul(tau, make_float2(sr, si));
-      for (int i = lane; i < m; i += 32) vc[i] = csub(vc[i], cmul(sv[i], ts));
-    }
-    __syncthreads();
-  }
-
-  // ---- 5. W = V diag(h) Vᴴ into A ------------------------------------------
-  for (int64_t q = tid; q < (int64_t)n * n; q += nt) {
-    const int a = (int)(q % n), b = (int)(q / n);
-    float wr = 0.f, wi = 0.f;
-    for (int i = 0; i < r; ++i) {
-      const float h = (float)hv[i];
-      const cf va = V[(int64_t)i * n + a], vb = V[(int64_t)i * n + b];
-      // h · va · conj(vb)
-      wr += h * (va.x * vb.x + va.y * vb.y);
-      wi += h * (va.y * vb.x - va.x * vb.y);
-    }
-    A[(int64_t)b * n + a] = make_float2(wr, wi);
   }
 }
 
@@ -688,7 +336,6 @@ PatchMap map_of(const ScaleGeom& g, const int N[3], int Nt, int64_t nvox) {
   return m;
 }
 
-size_t eig_smem(int n) { return (size_t)2 * n * sizeof(cf) + 32 * sizeof(double); }
 
 struct WorkPtrs {
   cf* gram;
@@ -699,11 +346,10 @@ struct WorkPtrs {
   cf* part;
 };
 
-// Gram → eig → (rebuild into out or pbuf) for all patches described by m.
-int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
-              const double* thr, int thr_per_patch, double lam, cf* out, int direct,
+// Gram matrices of all patches described by m into w.gram.
+int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
               cudaStream_t st, uint64_t* launches) {
-  if (launches) *launches += (nsplit > 1 ? 4 : 3);
+  if (launches) *launches += (nsplit > 1 ? 2 : 1);
   const int n = m.n;
   const int T = (n + kTile - 1) / kTile;
   const int ntri = T * (T + 1) / 2;
@@ -715,22 +361,31 @@ int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
     k_gram<<<dim3(ntri, (unsigned)np, 1), 256, 0, st>>>(in, m, w.gram, 1, m.L);
   }
   MSLR_CUDA_TRY(cudaGetLastError());
-  EigArgs ea;
-  ea.n = n;
-  ea.gram = w.gram;
-  ea.zv = w.zv;
-  ea.aux = w.aux;
-  ea.vecs = w.vecs;
-  ea.rank = w.rank;
-  ea.thr = thr;
-  ea.thr_per_patch = thr_per_patch;
-  ea.lam = lam;
-  k_eig<<<(unsigned)np, kEigThreads, eig_smem(n), st>>>(ea);
-  MSLR_CUDA_TRY(cudaGetLastError());
+  return MSLR_OK;
+}
+
+// out (image when direct, else per-patch buffer) = rebuild with W in w.gram.
+int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, cf* out,
+                 int direct, cudaStream_t st, uint64_t* launches) {
+  if (launches) *launches += 1;
+  const int n = m.n;
   k_rebuild<<<dim3((n + kTile - 1) / kTile, (m.L + kTile - 1) / kTile, (unsigned)np), 256, 0, st>>>(
       in, w.gram, m, out, direct);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
+}
+
+// Gram → eig → (rebuild into out or pbuf) for all patches described by m.
+int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
+              const double* thr, int thr_per_patch, double lam, cf* out, int direct,
+              cudaStream_t st, uint64_t* launches) {
+  int rc = svst_gram(in, m, np, w, nsplit, st, launches);
+  if (rc) return rc;
+  if (launches) *launches += 1;
+  rc = eig2_launch(m.n, np, w.gram, reinterpret_cast<cf*>(w.zv), reinterpret_cast<float*>(w.aux),
+                   w.rank, thr, thr_per_patch, lam, st);
+  if (rc) return rc;
+  return svst_rebuild(in, m, np, w, out, direct, st, launches);
 }
 
 int choose_split(int64_t np, int n, int L) {
@@ -847,21 +502,27 @@ int svst_setup(Ctx* c) {
     need = std::max(need, eig_work_bytes(g.Np, g.n, nsplit));
     if (!g.partition) pbuf = std::max(pbuf, (size_t)g.Np * c->Nt * g.p);
   }
-  c->svw.resize(1);
   int rc;
-  void* base = nullptr;
-  if ((rc = dalloc(c, &base, need))) return rc;
-  c->svw[0].gram = reinterpret_cast<cf*>(base);
+  // plain form: one workspace reused scale after scale; tuned form: one per
+  // scale, so that every patch of every scale is in flight in one eigen launch
+  const int nws = (c->form == MSLR_FORM_TUNED) ? c->Ns : 1;
+  c->svw.resize(nws);
+  for (int k = 0; k < nws; ++k) {
+    const ScaleGeom& g = c->scales[k];
+    const size_t bytes = (nws == 1) ? need
+                                    : eig_work_bytes(g.Np, g.n, choose_split(g.Np, g.n, g.L));
+    void* base = nullptr;
+    if ((rc = dalloc(c, &base, bytes))) return rc;
+    c->svw[k].gram = reinterpret_cast<cf*>(base);
+  }
   if (pbuf) {
     if ((rc = dalloc(c, (void**)&c->d_pbuf, pbuf * sizeof(cf)))) return rc;
     c->pbuf_elems = pbuf;
   }
   if ((rc = dalloc(c, (void**)&c->d_img_tmp, (size_t)c->Nt * c->nvox * sizeof(cf)))) return rc;
-  size_t maxsm = 0;
-  for (auto& g : c->scales) maxsm = std::max(maxsm, eig_smem(g.n));
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)std::max<size_t>(maxsm, 48 * 1024)));
-  return MSLR_OK;
+  int nmax = 1;
+  for (auto& g : c->scales) nmax = std::max(nmax, g.n);
+  return eig2_prepare(nmax);
 }
 
 int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_in, cf* img_out,
@@ -869,7 +530,7 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
   const ScaleGeom& g = c->scales[s];
   const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
   const int nsplit = choose_split(g.Np, g.n, g.L);
-  WorkPtrs w = carve(c->svw[0].gram, g.Np, g.n, nsplit);
+  WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? s : 0].gram, g.Np, g.n, nsplit);
   int rc;
   if (g.partition) {
     cf* dst = img_out;
@@ -883,6 +544,54 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
     k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, img_out);
     MSLR_CUDA_TRY(cudaGetLastError());
     c->launches += 1;
+  }
+  return MSLR_OK;
+}
+
+// g_prox of run_recon (scripts/reconstruct.jl:196-202) for every scale at once:
+// Grams of all scales, one eigen launch over every patch of every scale (the
+// global patch's eigensolve overlaps the local patches'), then the rebuilds.
+// Zin / Xout are (Ns, Nt, Nz, Ny, Nx); threshold of scale k = (*thr_dev)·λ_k.
+int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaStream_t st) {
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  if (c->svw.size() != (size_t)c->Ns) {
+    for (int k = 0; k < c->Ns; ++k) {
+      int rc = patch_svst(c, k, thr_dev, c->lambdas[k], Zin + k * E, Xout + k * E, st);
+      if (rc) return rc;
+    }
+    return MSLR_OK;
+  }
+  std::vector<EigSegment> segs(c->Ns);
+  std::vector<WorkPtrs> ws(c->Ns);
+  int rc;
+  for (int k = 0; k < c->Ns; ++k) {
+    const ScaleGeom& g = c->scales[k];
+    const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
+    const int nsplit = choose_split(g.Np, g.n, g.L);
+    ws[k] = carve(c->svw[k].gram, g.Np, g.n, nsplit);
+    if ((rc = svst_gram(Zin + k * E, m, g.Np, ws[k], nsplit, st, &c->launches))) return rc;
+    segs[k].n = g.n;
+    segs[k].np = g.Np;
+    segs[k].gram = ws[k].gram;
+    segs[k].zv = reinterpret_cast<cf*>(ws[k].zv);
+    segs[k].aux = ws[k].aux;
+    segs[k].rank = ws[k].rank;
+    segs[k].lam = c->lambdas[k];
+  }
+  if ((rc = eig_launch_multi(c->Ns, segs.data(), thr_dev, 0, st))) return rc;
+  c->launches += 1;
+  for (int k = 0; k < c->Ns; ++k) {
+    const ScaleGeom& g = c->scales[k];
+    const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
+    if (g.partition) {
+      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], Xout + k * E, 1, st, &c->launches)))
+        return rc;
+    } else {
+      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], c->d_pbuf, 0, st, &c->launches))) return rc;
+      k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, Xout + k * E);
+      MSLR_CUDA_TRY(cudaGetLastError());
+      c->launches += 1;
+    }
   }
   return MSLR_OK;
 }
@@ -949,8 +658,8 @@ int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* i
   m.tall = mrows >= ncols;
   m.batch = 1;
   m.mstride = (int64_t)mrows * ncols;
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)std::max<size_t>(eig_smem(1024), 48 * 1024)));
+  int rc = eig2_prepare(n);
+  if (rc) return rc;
   const cf* src = in;
   if (in == out) {
     MSLR_CUDA_TRY(cudaMemcpyAsync(stage, in, (size_t)batch * mrows * ncols * sizeof(cf),
