@@ -34,7 +34,7 @@ int patches_op(const int N[3], int Nt, const int ps[3], const int ss[3], const c
                bool to_patches, cudaStream_t st);
 size_t svst_batch_bytes(int mrows, int ncols, int batch);
 int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* in, cf* out,
-               void* ws, size_t ws_bytes, cudaStream_t st);
+               void* ws, size_t ws_bytes, int form, cudaStream_t st);
 int svst_batch_noalloc(int mrows, int ncols, int batch, const double* betas, const cf* in, cf* out,
                        cudaStream_t st);
 
@@ -135,9 +135,9 @@ int mslr_svst_batch(int32_t m, int32_t n, int32_t batch, const double* betas, co
   for (int b = 0; b < batch; ++b)
     if (!(betas[b] >= 0.0) || !std::isfinite(betas[b]))
       return fail(MSLR_ERR_ARG, "thresholds must be finite and non-negative");
-  (void)form;
+  if (form != MSLR_FORM_PLAIN && form != MSLR_FORM_TUNED) return fail(MSLR_ERR_ARG, "unknown form");
   return svst_batch(m, n, batch, betas, reinterpret_cast<const cf*>(in), reinterpret_cast<cf*>(out),
-                    workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
+                    workspace, workspace_bytes, form, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int mslr_svst_batch_noalloc(int32_t m, int32_t n, int32_t batch, const double* betas,

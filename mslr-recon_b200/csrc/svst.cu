@@ -24,6 +24,7 @@
 #include <mutex>
 
 #include "internal.h"
+#include "patchmap.cuh"
 
 namespace mslr {
 
@@ -31,53 +32,6 @@ namespace {
 
 constexpr int kTile = 64;
 constexpr int kKc = 16;
-
-// Device-side addressing of patch elements.  Element (l, t) of patch ip —
-// l the in-patch voxel (x fastest), t the frame — lives at
-//   image mode: origin(ip) + lx + Nx (ly + Ny lz) + t·nvox
-//   batch mode: ip·mstride + l + t·m        (column-major m × Nt matrices)
-struct PatchMap {
-  int Nx, Ny, Nz;
-  int64_t nvox;
-  int Nt;
-  int psx, psy, psz;
-  int nx, ny, nz;     // patches per dim
-  const int* starts;  // nx x-starts, ny y-starts, nz z-starts
-  int p, n, L;
-  int tall;
-  int batch;
-  int64_t mstride;
-};
-
-__device__ __forceinline__ int64_t patch_origin(const PatchMap& m, int64_t ip) {
-  if (m.batch) return ip * m.mstride;
-  const int ix = (int)(ip % m.nx);
-  const int iy = (int)((ip / m.nx) % m.ny);
-  const int iz = (int)(ip / ((int64_t)m.nx * m.ny));
-  const int sx = m.starts[ix], sy = m.starts[m.nx + iy], sz = m.starts[m.nx + m.ny + iz];
-  return sx + (int64_t)m.Nx * (sy + (int64_t)m.Ny * sz);
-}
-
-__device__ __forceinline__ int64_t patch_off(const PatchMap& m, int l) {
-  if (m.batch) return l;
-  const int lx = l % m.psx;
-  const int r = l / m.psx;
-  const int ly = r % m.psy;
-  const int lz = r / m.psy;
-  return lx + (int64_t)m.Nx * (ly + (int64_t)m.Ny * lz);
-}
-
-__device__ __forceinline__ int64_t tstride(const PatchMap& m) { return m.batch ? (int64_t)m.p : m.nvox; }
-
-// M[a][l] of patch with origin `org`
-__device__ __forceinline__ cf m_elem(const PatchMap& m, const cf* __restrict__ img, int64_t org,
-                                     int a, int l) {
-  if (m.tall) {
-    const cf v = img[org + patch_off(m, l) + (int64_t)a * tstride(m)];
-    return cconj(v);
-  }
-  return img[org + patch_off(m, a) + (int64_t)l * tstride(m)];
-}
 
 // ---------------------------------------------------------------------------
 // Gram: G[a][b] = Σ_l M[a][l] conj(M[b][l]) on lower-triangle 64×64 tiles.
@@ -347,27 +301,31 @@ struct WorkPtrs {
 };
 
 // Gram matrices of all patches described by m into w.gram.
-int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
+// Tensor cores (tc, tuned form: split-precision BF16 mma) or FP32 SIMT.
+int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit, bool tc,
               cudaStream_t st, uint64_t* launches) {
   if (launches) *launches += (nsplit > 1 ? 2 : 1);
   const int n = m.n;
   const int T = (n + kTile - 1) / kTile;
   const int ntri = T * (T + 1) / 2;
-  if (nsplit > 1) {
-    const int lchunk = ((m.L + nsplit - 1) / nsplit + kKc - 1) / kKc * kKc;
-    k_gram<<<dim3(ntri, (unsigned)np, nsplit), 256, 0, st>>>(in, m, w.part, nsplit, lchunk);
-    k_gram_reduce<<<592, 256, 0, st>>>(w.part, w.gram, nsplit, (int64_t)n * n);
+  const int lchunk = (nsplit > 1) ? ((m.L + nsplit - 1) / nsplit + 31) / 32 * 32 : m.L;
+  cf* dst = (nsplit > 1) ? w.part : w.gram;
+  if (tc) {
+    int rc = gram_mma_launch(in, m, np, dst, nsplit, lchunk, st);
+    if (rc) return rc;
   } else {
-    k_gram<<<dim3(ntri, (unsigned)np, 1), 256, 0, st>>>(in, m, w.gram, 1, m.L);
+    k_gram<<<dim3(ntri, (unsigned)np, nsplit), 256, 0, st>>>(in, m, dst, nsplit, lchunk);
   }
+  if (nsplit > 1) k_gram_reduce<<<592, 256, 0, st>>>(w.part, w.gram, nsplit, (int64_t)n * n);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
 }
 
 // out (image when direct, else per-patch buffer) = rebuild with W in w.gram.
 int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, cf* out,
-                 int direct, cudaStream_t st, uint64_t* launches) {
+                 int direct, bool tc, cudaStream_t st, uint64_t* launches) {
   if (launches) *launches += 1;
+  if (tc) return rebuild_mma_launch(in, w.gram, m, np, out, direct, st);
   const int n = m.n;
   k_rebuild<<<dim3((n + kTile - 1) / kTile, (m.L + kTile - 1) / kTile, (unsigned)np), 256, 0, st>>>(
       in, w.gram, m, out, direct);
@@ -377,15 +335,15 @@ int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w,
 
 // Gram → eig → (rebuild into out or pbuf) for all patches described by m.
 int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
-              const double* thr, int thr_per_patch, double lam, cf* out, int direct,
+              const double* thr, int thr_per_patch, double lam, cf* out, int direct, bool tc,
               cudaStream_t st, uint64_t* launches) {
-  int rc = svst_gram(in, m, np, w, nsplit, st, launches);
+  int rc = svst_gram(in, m, np, w, nsplit, tc, st, launches);
   if (rc) return rc;
   if (launches) *launches += 1;
   rc = eig2_launch(m.n, np, w.gram, reinterpret_cast<cf*>(w.zv), reinterpret_cast<float*>(w.aux),
                    w.rank, thr, thr_per_patch, lam, st);
   if (rc) return rc;
-  return svst_rebuild(in, m, np, w, out, direct, st, launches);
+  return svst_rebuild(in, m, np, w, out, direct, tc, st, launches);
 }
 
 int choose_split(int64_t np, int n, int L) {
@@ -531,16 +489,20 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
   const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
   const int nsplit = choose_split(g.Np, g.n, g.L);
   WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? s : 0].gram, g.Np, g.n, nsplit);
+  const bool tc = (c->form == MSLR_FORM_TUNED);
   int rc;
   if (g.partition) {
     cf* dst = img_out;
     if (img_in == img_out) dst = c->d_img_tmp;   // Gram/rebuild read the input throughout
-    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, dst, 1, st, &c->launches))) return rc;
+    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, dst, 1, tc, st, &c->launches)))
+      return rc;
     if (dst != img_out)
       MSLR_CUDA_TRY(cudaMemcpyAsync(img_out, dst, (size_t)c->Nt * c->nvox * sizeof(cf),
                                     cudaMemcpyDeviceToDevice, st));
   } else {
-    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, c->d_pbuf, 0, st, &c->launches))) return rc;
+    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, c->d_pbuf, 0, tc, st,
+                        &c->launches)))
+      return rc;
     k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, img_out);
     MSLR_CUDA_TRY(cudaGetLastError());
     c->launches += 1;
@@ -569,7 +531,7 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
     const int nsplit = choose_split(g.Np, g.n, g.L);
     ws[k] = carve(c->svw[k].gram, g.Np, g.n, nsplit);
-    if ((rc = svst_gram(Zin + k * E, m, g.Np, ws[k], nsplit, st, &c->launches))) return rc;
+    if ((rc = svst_gram(Zin + k * E, m, g.Np, ws[k], nsplit, true, st, &c->launches))) return rc;
     segs[k].n = g.n;
     segs[k].np = g.Np;
     segs[k].gram = ws[k].gram;
@@ -584,10 +546,11 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     const ScaleGeom& g = c->scales[k];
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
     if (g.partition) {
-      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], Xout + k * E, 1, st, &c->launches)))
+      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], Xout + k * E, 1, true, st, &c->launches)))
         return rc;
     } else {
-      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], c->d_pbuf, 0, st, &c->launches))) return rc;
+      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], c->d_pbuf, 0, true, st, &c->launches)))
+        return rc;
       k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, Xout + k * E);
       MSLR_CUDA_TRY(cudaGetLastError());
       c->launches += 1;
@@ -630,7 +593,7 @@ size_t svst_batch_bytes(int mrows, int ncols, int batch) {
 }
 
 int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* in, cf* out,
-               void* ws, size_t ws_bytes, cudaStream_t st) {
+               void* ws, size_t ws_bytes, int form, cudaStream_t st) {
   const int n = std::min(mrows, ncols);
   const size_t need = svst_batch_bytes(mrows, ncols, batch);
   if (ws_bytes < need) return fail(MSLR_ERR_ARG, "workspace too small for mslr_svst_batch");
@@ -666,7 +629,8 @@ int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* i
                                   cudaMemcpyDeviceToDevice, st));
     src = stage;
   }
-  return svst_core(src, m, batch, w, 1, d_beta, 1, 1.0, out, 1, st, nullptr);
+  return svst_core(src, m, batch, w, 1, d_beta, 1, 1.0, out, 1, form == MSLR_FORM_TUNED, st,
+                   nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -711,7 +675,7 @@ int svst_batch_noalloc(int mrows, int ncols, int batch, const double* betas, con
   // No part of the scratch has to start at zero: every stage writes what the
   // next one reads, so the previous call's contents are simply overwritten.
   return svst_batch(mrows, ncols, batch, betas, in, out, scratch, (size_t)MSLR_NOALLOC_SCRATCH_BYTES,
-                    st);
+                    MSLR_FORM_TUNED, st);
 }
 
 }  // namespace mslr

@@ -74,9 +74,13 @@ def test_recombine_matches_reference_order(torch, M, N, ps, ss):
 
 
 # --- SVST ------------------------------------------------------------------------
+SVST_TOL = {"plain": 2e-5, "tuned": 1e-4}   # FP32 SIMT; split-precision BF16x3 tensor cores
+
+
+@pytest.mark.parametrize("form", ["plain", "tuned"])
 @pytest.mark.parametrize("m,n,batch", [(40, 12, 5), (12, 40, 5), (216, 64, 7), (64, 216, 3), (1000, 300, 2),
                                        (1, 30, 4), (30, 1, 4)])
-def test_svst_batch_vs_oracle(torch, M, m, n, batch):
+def test_svst_batch_vs_oracle(torch, M, m, n, batch, form):
     rng = np.random.default_rng(m * 1000 + n)
     X = (rng.standard_normal((batch, m, n)) + 1j * rng.standard_normal((batch, m, n))).astype(np.complex64)
     # low-rank + noise so that thresholds land inside the spectrum
@@ -92,27 +96,28 @@ def test_svst_batch_vs_oracle(torch, M, m, n, batch):
         X[2] = 0
         betas[2] = 1.0
     cm = np.ascontiguousarray(np.transpose(X, (0, 2, 1)))   # column-major storage
-    out = M.svst_batch(dev(torch, cm), m, n, betas).cpu().numpy()
+    from mslr_recon_b200.context import FORMS
+    out = M.svst_batch(dev(torch, cm), m, n, betas, form=FORMS[form]).cpu().numpy()
     out = np.transpose(out, (0, 2, 1))
     for b in range(batch):
         ref = O.svst(X[b].astype(np.complex128), betas[b])
         if np.linalg.norm(ref) == 0:
             assert np.all(out[b] == 0)
         else:
-            assert rel(out[b], ref) < 2e-5, (b, rel(out[b], ref))
+            assert rel(out[b], ref) < SVST_TOL[form], (b, rel(out[b], ref))
 
 
 def test_svst_single_matrix(torch, M):
     rng = np.random.default_rng(12)
     X = (rng.standard_normal((50, 20)) + 1j * rng.standard_normal((50, 20))).astype(np.complex64)
     out = M.SVST(dev(torch, X), 4.0).cpu().numpy()
-    assert rel(out, O.svst(X.astype(np.complex128), 4.0)) < 2e-5
+    assert rel(out, O.svst(X.astype(np.complex128), 4.0)) < SVST_TOL["tuned"]   # default form
 
 
 @pytest.mark.parametrize("k", [0, 1, 2])
 def test_patch_svst_golden(torch, M, gold, k):
     out = M.patchSVST(dev(torch, gold["x"]), 3.0, PATCHES[k], STRIDES[k]).cpu().numpy()
-    assert rel(out, gold[f"svst{k}"]) < 2e-5
+    assert rel(out, gold[f"svst{k}"]) < SVST_TOL["tuned"]   # default form
 
 
 # --- SENSE -------------------------------------------------------------------------
