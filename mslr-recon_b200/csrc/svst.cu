@@ -310,7 +310,7 @@ int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
   const int ntri = T * (T + 1) / 2;
   const int lchunk = (nsplit > 1) ? ((m.L + nsplit - 1) / nsplit + 31) / 32 * 32 : m.L;
   cf* dst = (nsplit > 1) ? w.part : w.gram;
-  if (tc) {
+  if (tc && mma_supported(m)) {
     int rc = gram_mma_launch(in, m, np, dst, nsplit, lchunk, st);
     if (rc) return rc;
   } else {
@@ -325,7 +325,7 @@ int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
 int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, cf* out,
                  int direct, bool tc, cudaStream_t st, uint64_t* launches) {
   if (launches) *launches += 1;
-  if (tc) return rebuild_mma_launch(in, w.gram, m, np, out, direct, st);
+  if (tc && mma_supported(m)) return rebuild_mma_launch(in, w.gram, m, np, out, direct, st);
   const int n = m.n;
   k_rebuild<<<dim3((n + kTile - 1) / kTile, (m.L + kTile - 1) / kTile, (unsigned)np), 256, 0, st>>>(
       in, w.gram, m, out, direct);
