@@ -346,6 +346,8 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
   if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
   if (herr & 4)
     return ctx_fail(ctx, fail(MSLR_ERR_NONFINITE, "non-finite value in the POGM restart sums"));
+  if (herr & 8)
+    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a device-side wait for a bulk copy timed out"));
   return MSLR_OK;
 }
 

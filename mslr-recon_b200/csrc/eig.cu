@@ -1,18 +1,22 @@
 // eig.cu — per-patch Hermitian eigen stage of the patch SVST (sm_100a).
 //
 // For each patch Gram matrix G (n × n, Hermitian, column-major, FP32 complex)
-// and threshold β this computes the rebuild matrix
-//     W = V diag(h) Vᴴ,   h_i = max(√λ_i − β, 0) / √λ_i,
-// over the eigenpairs (λ_i, v_i) of G with λ_i > β² — the SVST of the patch
-// (src/recon.jl:183-211) expressed through its Gram matrix.  One CTA per
-// patch — 384 threads when n <= 384 (two patches per SM, so one patch's
-// latency-bound phases overlap the other's), else 1024; one launch may cover
-// several segments (the patches of several scales, each with its own n and
-// λ_k).  The matrix lives in global memory (L2):
+// and threshold β this computes the scaled eigenvector matrix
+//     Ṽ = V diag(√h),   h_i = max(√λ_i − β, 0) / √λ_i,
+// over the eigenpairs (λ_i, v_i) of G with λ_i > β², so that the rebuild
+// matrix of the patch SVST (src/recon.jl:183-211, expressed through its Gram
+// matrix) is W = Ṽ Ṽᴴ — one more Gram product, formed by the batched Gram
+// kernels after this launch.  One CTA per patch — 384 threads when n <= 384
+// (two patches per SM, so one patch's latency-bound phases overlap the
+// other's), else 1024; one launch may cover several segments (the patches of
+// several scales, each with its own n and λ_k).  The matrix lives in global
+// memory (L2); only its lower triangle is read or written:
 //   1. Householder tridiagonalisation G = Q T Qᴴ (FP32).  Each step applies
 //      the previous step's rank-2 update on the fly while forming the next
-//      matrix-vector product, so the trailing block is streamed once per step
-//      (thread i owns row i; column-major reads are coalesced).
+//      Hermitian matrix-vector product over 32 × 32 tiles of the trailing
+//      lower triangle (one warp per tile: row sums per lane, column sums by a
+//      shuffle transpose-reduction), so the trailing triangle is streamed
+//      once per step and the working set of ~300 resident patches stays in L2.
 //   2. Eigenvalues of T above β² by bisection on FP64 Sturm counts, one
 //      thread per eigenvalue.
 //   3. Eigenvectors of T by FP64 twisted factorisation, one thread per
@@ -21,10 +25,10 @@
 //   4. V = Q Z with the reflectors applied 16 at a time in compact WY form
 //      (Q_b = I − Y T Yᴴ); thread i keeps vector i's block coefficients in
 //      registers, so the update needs no cross-thread reduction.
-//   5. W = V diag(h) Vᴴ on 4×4 register tiles of the lower triangle,
-//      mirrored.
-// Zero patches give no eigenvalue above β² and W = 0 (the reference's
-// zero-norm skip, src/recon.jl:185).
+//   5. Ṽ written as conj(V) diag(√h) in row-major order ([row][vector]),
+//      columns beyond the rank set to zero.
+// Zero patches give no eigenvalue above β² and Ṽ = 0, hence W = 0 (the
+// reference's zero-norm skip, src/recon.jl:185).
 #include <cmath>
 
 #include "internal.h"
@@ -36,7 +40,6 @@ namespace {
 constexpr int kT = 1024;   // most threads per CTA (one row / eigenvalue per thread)
 constexpr int kSmallT = 384;   // CTA size for n <= 384: two patches share an SM
 constexpr int kNb = 16;    // reflectors per WY block
-constexpr int kVc = 16;    // eigenvectors per W staging chunk
 
 __device__ __forceinline__ float warp_sum(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -87,8 +90,8 @@ struct Seg {
   int n;
   int64_t first;   // first block of the segment
   int64_t np;      // patches
-  cf* gram;        // np × n × n: G in, Householder vectors, then W out
-  cf* zv;          // np × n × n: eigenvectors, [row j][vector i], i fastest
+  cf* gram;        // np × n × n: G in (lower triangle), Householder vectors out
+  cf* zv;          // np × n × n: eigenvectors, [row j][vector i], i fastest; Ṽ out
   double* aux;     // np × n × n: FP64 pivots of the twisted factorisations
   int* rank;       // np
   double lam;      // threshold multiplier of the segment (λ_k)
@@ -103,12 +106,13 @@ struct EigArgs {
   int thr_per_patch;
 };
 
+// vectors are padded to n + 32 entries (zero tails) so 32-wide tiles read them in bounds
 size_t smem_bytes(int n) {
-  const size_t vecs = 3 * (size_t)n * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
+  const size_t np = (size_t)n + 32;
+  const size_t vecs = 4 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
                       3 * (size_t)n * sizeof(float) + 64 * sizeof(float) + 64 * sizeof(double);
   const size_t wy = (size_t)n * kNb * sizeof(cf) + 2 * kNb * kNb * sizeof(cf);
-  const size_t wt = (size_t)n * kVc * sizeof(cf);
-  return vecs + std::max(wy, wt) + 128;
+  return vecs + wy + 128;
 }
 
 template <int MAXT, int MINB>
@@ -125,16 +129,18 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   cf* Z = S.zv + ip * (int64_t)n * n;
   double* AUX = S.aux + ip * (int64_t)n * n;
 
-  // shared layout (8-byte aligned pieces first)
+  // shared layout (8-byte aligned pieces first); complex vectors hold n + 32 entries
+  const int npad = n + 32;
   double* dd = reinterpret_cast<double*>(smraw);   // diagonal        [n]
   double* ee = dd + n;                              // off-diagonal    [n]
   double* ee2 = ee + n;                             // e²              [n]
   double* lam = ee2 + n;                            // eigenvalues     [n]
   double* redd = lam + n;                           // 64 doubles
-  cf* sv = reinterpret_cast<cf*>(redd + 64);        // v of this step  [n]
-  cf* svp = sv + n;                                 // previous v      [n]
-  cf* swp = svp + n;                                // previous w      [n]
-  float* hv = reinterpret_cast<float*>(swp + n);    // h               [n]
+  cf* sv = reinterpret_cast<cf*>(redd + 64);        // v of this step  [npad]
+  cf* svp = sv + npad;                              // previous v      [npad]
+  cf* swp = svp + npad;                             // previous w      [npad]
+  cf* ys = swp + npad;                              // y accumulator   [npad]
+  float* hv = reinterpret_cast<float*>(ys + npad);  // h               [n]
   float* taur = hv + n;                             // τ               [n]
   float* taui = taur + n;                           //                 [n]
   float* red0 = taui + n;                           // 2 × 32 floats
@@ -146,14 +152,18 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
 
   const double beta_d = g.thr[g.thr_per_patch ? (int64_t)blockIdx.x : 0] * S.lam;
   const float beta = (float)beta_d;
+  (void)beta;
 
   // ---- 1. tridiagonalisation with delayed rank-2 updates ---------------------
-  for (int q = tid; q < n; q += kT) {
+  for (int q = tid; q < npad; q += kT) {
+    sv[q] = make_float2(0.f, 0.f);
     svp[q] = make_float2(0.f, 0.f);
     swp[q] = make_float2(0.f, 0.f);
+    ys[q] = make_float2(0.f, 0.f);
   }
   __syncthreads();
   const int i = tid;   // row owned by this thread (n <= kT)
+  const int warp = tid >> 5, lane = tid & 31, nwarp = kT >> 5;
   for (int k = 0; k < n - 1; ++k) {
     // current column k and diagonal k: stored − (vp wpᴴ + wp vpᴴ)
     cf x = make_float2(0.f, 0.f);
@@ -164,7 +174,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     }
     const cf vpk = svp[k], wpk = swp[k];
     if (i >= k && i < n) {
-      x = A[(int64_t)k * n + i];
+      x = __ldcg(A + (int64_t)k * n + i);
       x = csub(x, cadd(cmul(vpi, cconj(wpk)), cmul(wpi, cconj(vpk))));
       if (i == k) dd[k] = (double)x.x;
     }
@@ -209,38 +219,103 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     }
     if (i < n) sv[i] = vi;
     __syncthreads();
-    // fused: A22 ← A22 − (vp wpᴴ + wp vpᴴ);  y = A22 v.  Loads are issued in
-    // batches of kB before the corresponding stores, so a thread keeps kB
-    // L2 requests in flight instead of one.
-    float yr = 0.f, yi = 0.f;
-    if (i >= k + 1 && i < n) {
-      constexpr int kB = 8;
-      cf* col = A + (int64_t)(k + 1) * n + i;
-      int j = k + 1;
-      for (; j + kB <= n; j += kB, col += (int64_t)kB * n) {
-        cf a[kB];
+    // fused over the trailing lower triangle [o, n)²: A22 ← A22 − (vp wpᴴ + wp vpᴴ)
+    // and y = A22 v (Hermitian: element (r, c), r > c, also gives y_c += conj(a) v_r).
+    {
+      const int o = k + 1;
+      const int T = (n - o + 31) >> 5;
+      const int ntile = T * (T + 1) / 2;
+      for (int t = warp; t < ntile; t += nwarp) {
+        int I = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+        while ((I + 1) * (I + 2) / 2 <= t) ++I;
+        while (I * (I + 1) / 2 > t) --I;
+        const int J = t - I * (I + 1) / 2;
+        const bool diag = (I == J);
+        const int row = o + I * 32 + lane;
+        const bool rowok = row < n;
+        const int rr = rowok ? row : n - 1;
+        const cf vpr = svp[rr], wpr = swp[rr];
+        const cf vr = rowok ? sv[rr] : make_float2(0.f, 0.f);
+        float yr = 0.f, yim = 0.f;
+        const int j0 = o + J * 32;
+        cf* col0 = A + (int64_t)j0 * n + rr;
+        for (int g8 = 0; g8 < 4; ++g8) {
+          const int jb = j0 + g8 * 8;
+          if (jb >= n) break;
+          cf a[8];
 #pragma unroll
-        for (int b = 0; b < kB; ++b) a[b] = __ldcg(col + (int64_t)b * n);
+          for (int b = 0; b < 8; ++b) {
+            const int j = jb + b;
+            const bool ok = rowok && j < n && (!diag || row >= j);
+            a[b] = ok ? __ldcg(col0 + (int64_t)(g8 * 8 + b) * n) : make_float2(0.f, 0.f);
+          }
+          float cr[8], ci[8];
 #pragma unroll
-        for (int b = 0; b < kB; ++b) {
-          const cf vpj = svp[j + b], wpj = swp[j + b], vj = sv[j + b];
-          a[b].x -= (vpi.x * wpj.x + vpi.y * wpj.y) + (wpi.x * vpj.x + wpi.y * vpj.y);
-          a[b].y -= (vpi.y * wpj.x - vpi.x * wpj.y) + (wpi.y * vpj.x - wpi.x * vpj.y);
-          yr += a[b].x * vj.x - a[b].y * vj.y;
-          yi += a[b].x * vj.y + a[b].y * vj.x;
+          for (int b = 0; b < 8; ++b) {
+            const int j = jb + b;
+            const bool ok = rowok && j < n && (!diag || row >= j);
+            const cf vpj = svp[j], wpj = swp[j], vj = sv[j];
+            cf e = a[b];
+            e.x -= (vpr.x * wpj.x + vpr.y * wpj.y) + (wpr.x * vpj.x + wpr.y * vpj.y);
+            e.y -= (vpr.y * wpj.x - vpr.x * wpj.y) + (wpr.y * vpj.x - wpr.x * vpj.y);
+            if (!ok) e = make_float2(0.f, 0.f);
+            a[b] = e;
+            yr += e.x * vj.x - e.y * vj.y;
+            yim += e.x * vj.y + e.y * vj.x;
+            const bool low = !diag || row > j;   // strictly below the diagonal
+            cr[b] = low ? (e.x * vr.x + e.y * vr.y) : 0.f;
+            ci[b] = low ? (e.x * vr.y - e.y * vr.x) : 0.f;
+          }
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            const int j = jb + b;
+            if (rowok && j < n && (!diag || row >= j)) col0[(int64_t)(g8 * 8 + b) * n] = a[b];
+          }
+          // column sums over the 32 lanes: lane l ends with the sum of column l/4
+          const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float sr_ = h16 ? cr[q] : cr[q + 4], si_ = h16 ? ci[q] : ci[q + 4];
+            const float kr = h16 ? cr[q + 4] : cr[q], ki = h16 ? ci[q + 4] : ci[q];
+            cr[q] = kr + __shfl_xor_sync(0xffffffffu, sr_, 16);
+            ci[q] = ki + __shfl_xor_sync(0xffffffffu, si_, 16);
+          }
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const float sr_ = h8 ? cr[q] : cr[q + 2], si_ = h8 ? ci[q] : ci[q + 2];
+            const float kr = h8 ? cr[q + 2] : cr[q], ki = h8 ? ci[q + 2] : ci[q];
+            cr[q] = kr + __shfl_xor_sync(0xffffffffu, sr_, 8);
+            ci[q] = ki + __shfl_xor_sync(0xffffffffu, si_, 8);
+          }
+          {
+            const float sr_ = h4 ? cr[0] : cr[1], si_ = h4 ? ci[0] : ci[1];
+            const float kr = h4 ? cr[1] : cr[0], ki = h4 ? ci[1] : ci[0];
+            cr[0] = kr + __shfl_xor_sync(0xffffffffu, sr_, 4);
+            ci[0] = ki + __shfl_xor_sync(0xffffffffu, si_, 4);
+          }
+          cr[0] += __shfl_xor_sync(0xffffffffu, cr[0], 2);
+          ci[0] += __shfl_xor_sync(0xffffffffu, ci[0], 2);
+          cr[0] += __shfl_xor_sync(0xffffffffu, cr[0], 1);
+          ci[0] += __shfl_xor_sync(0xffffffffu, ci[0], 1);
+          const int jc = jb + (lane >> 2);
+          if (jc < n) {
+            if ((lane & 3) == 0) atomicAdd(&ys[jc].x, cr[0]);
+            else if ((lane & 3) == 1) atomicAdd(&ys[jc].y, ci[0]);
+          }
         }
-#pragma unroll
-        for (int b = 0; b < kB; ++b) col[(int64_t)b * n] = a[b];
+        if (rowok) {
+          atomicAdd(&ys[row].x, yr);
+          atomicAdd(&ys[row].y, yim);
+        }
       }
-      for (; j < n; ++j, col += n) {
-        cf a = __ldcg(col);
-        const cf vpj = svp[j], wpj = swp[j], vj = sv[j];
-        a.x -= (vpi.x * wpj.x + vpi.y * wpj.y) + (wpi.x * vpj.x + wpi.y * vpj.y);
-        a.y -= (vpi.y * wpj.x - vpi.x * wpj.y) + (wpi.y * vpj.x - wpi.x * vpj.y);
-        *col = a;
-        yr += a.x * vj.x - a.y * vj.y;
-        yi += a.x * vj.y + a.y * vj.x;
-      }
+    }
+    __syncthreads();
+    float yr = 0.f, yi = 0.f;
+    if (i < n) {
+      const cf y = ys[i];
+      yr = y.x;
+      yi = y.y;
+      ys[i] = make_float2(0.f, 0.f);   // cleared for the next step (two barriers ahead)
     }
     // vᴴ y (real for Hermitian A)
     const float vy = block_sum((i >= k + 1 && i < n) ? (vi.x * yr + vi.y * yi) : 0.f,
@@ -258,7 +333,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     __syncthreads();
   }
   if (i == n - 1) {
-    cf x = A[(int64_t)(n - 1) * n + (n - 1)];
+    cf x = __ldcg(A + (int64_t)(n - 1) * n + (n - 1));
     const cf vpk = svp[n - 1], wpk = swp[n - 1];
     x = csub(x, cadd(cmul(vpk, cconj(wpk)), cmul(wpk, cconj(vpk))));
     dd[n - 1] = (double)x.x;
@@ -309,7 +384,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   }
   __syncthreads();
   if (r == 0) {
-    for (int64_t q = tid; q < (int64_t)n * n; q += kT) A[q] = make_float2(0.f, 0.f);
+    for (int64_t q = tid; q < (int64_t)n * n; q += kT) Z[q] = make_float2(0.f, 0.f);
     return;
   }
 
@@ -490,65 +565,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     __syncthreads();
   }
 
-  // ---- 5. W = V diag(h) Vᴴ, lower 4×4 tiles, mirrored into A ------------------
-  cf* sVc = sY;   // staging: sVc[row*kVc + c] = √h_c · V[row][i0 + c]
-  const int nt4 = (n + 3) / 4;
-  const int ntiles = nt4 * (nt4 + 1) / 2;
-  for (int tile0 = 0; tile0 < ntiles; tile0 += kT) {
-    const int tile = tile0 + tid;
-    int ta = 0, tb = 0;
-    const bool act = tile < ntiles;
-    if (act) {
-      ta = (int)((sqrtf(8.f * tile + 1.f) - 1.f) * 0.5f);
-      while ((ta + 1) * (ta + 2) / 2 <= tile) ++ta;
-      while (ta * (ta + 1) / 2 > tile) --ta;
-      tb = tile - ta * (ta + 1) / 2;
-    }
-    cf acc[4][4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[p][q] = make_float2(0.f, 0.f);
-    for (int i0 = 0; i0 < r; i0 += kVc) {
-      const int cnt = min(kVc, r - i0);
-      __syncthreads();
-      for (int q = tid; q < n * kVc; q += kT) {
-        const int row = q / kVc, c = q - row * kVc;
-        sVc[q] = (c < cnt) ? cscale(Z[(int64_t)row * n + i0 + c], sqrtf(hv[i0 + c]))
-                           : make_float2(0.f, 0.f);
-      }
-      __syncthreads();
-      if (act) {
-        for (int c = 0; c < cnt; ++c) {
-          cf va[4], vb[4];
-#pragma unroll
-          for (int p = 0; p < 4; ++p) {
-            const int a = ta * 4 + p, b = tb * 4 + p;
-            va[p] = (a < n) ? sVc[a * kVc + c] : make_float2(0.f, 0.f);
-            vb[p] = (b < n) ? sVc[b * kVc + c] : make_float2(0.f, 0.f);
-          }
-#pragma unroll
-          for (int p = 0; p < 4; ++p)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {   // va · conj(vb)
-              acc[p][q].x += va[p].x * vb[q].x + va[p].y * vb[q].y;
-              acc[p][q].y += va[p].y * vb[q].x - va[p].x * vb[q].y;
-            }
-        }
-      }
-    }
-    __syncthreads();
-    if (act) {
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int a = ta * 4 + p, b = tb * 4 + q;
-          if (a < n && b < n) {
-            A[(int64_t)b * n + a] = acc[p][q];
-            A[(int64_t)a * n + b] = cconj(acc[p][q]);
-          }
-        }
+  // ---- 5. Ṽ = conj(V) diag(√h), columns >= r zero ------------------------------
+  for (int c = tid; c < n; c += kT) {
+    const float sh = (c < r) ? sqrtf(hv[c]) : 0.f;
+    for (int row = 0; row < n; ++row) {
+      const cf z = (c < r) ? Z[(int64_t)row * n + c] : make_float2(0.f, 0.f);
+      Z[(int64_t)row * n + c] = make_float2(z.x * sh, -z.y * sh);
     }
   }
 }

@@ -66,6 +66,12 @@ struct Ctx {
   bool fast = false;
   alignas(16) unsigned char fplan_raw[3 * 256];   // fast::FPlan x, y, z (fft_fast.cuh)
   int Ffast = 1;
+  int nsm = 148;          // SMs of the bound device (persistent grids)
+  bool zpre = false;      // z kernels with prefetched slabs fit in shared memory
+  bool xypers = false;    // persistent plane kernel with a prefetch buffer fits
+  bool spec = false;      // shape-specialised kernels (sense_spec.cu) exist for N
+  int spec_xy_ctas = 0;   // resident CTAs of the specialised plane kernel
+  int spec_zfwd_ctas = 0; // resident CTAs of the specialised forward z kernel
 
   // POGM
   cf* d_U = nullptr;   // (Ns, Nt, nvox)
@@ -112,6 +118,11 @@ int normal_op_fast(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
 int sense_forward_fast(Ctx* c, const cf* x, cf* y, cudaStream_t st);
 int sense_adjoint_fast(Ctx* c, const cf* y, cf* x, cudaStream_t st);
 
+// ---- sense_spec.cu (tuned form, compiled shapes) ---------------------------------
+bool sense_spec_setup(Ctx* c);
+int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
+                   cudaStream_t st);
+
 // ---- svst.cu -----------------------------------------------------------------
 int svst_setup(Ctx* c);   // workspaces (create time)
 // img_out = patchSVST(img_in) for scale s with threshold (*thr_dev) * lam
@@ -127,8 +138,8 @@ void geom_free(ScaleGeom* g);
 struct EigSegment {
   int n;
   int64_t np;
-  cf* gram;      // np × n × n: Gram in, W out
-  cf* zv;        // np × n × n scratch
+  cf* gram;      // np × n × n: Gram in (lower triangle read), Householder vectors out
+  cf* zv;        // np × n × n: Ṽ = V diag(√h) out, conjugated, row-major (W = Ṽ Ṽᴴ)
   double* aux;   // np × n × n scratch
   int* rank;     // np
   double lam;

@@ -341,8 +341,10 @@ int sense_setup_tables(Ctx* c) {
   c->nwords = (int)((c->nvox + 31) / 32);
   // tuned form: register-resident kernels when every axis has a fast plan;
   // one frame per chunk so that the chunk's per-coil k-space can stay in L2
-  if (c->form == MSLR_FORM_TUNED)
+  if (c->form == MSLR_FORM_TUNED) {
     c->fast = sense_fast_setup(c);
+    c->spec = c->fast && sense_spec_setup(c);
+  }
   c->Ffast = 1;
   return MSLR_OK;
 }
@@ -421,6 +423,7 @@ int sense_adjoint(Ctx* c, const cf* y, cf* x, cudaStream_t st) {
 
 int normal_op(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
               cudaStream_t st) {
+  if (c->spec) return normal_op_spec(c, X, ns, sstride, g, subtract, st);
   if (c->fast) return normal_op_fast(c, X, ns, sstride, g, subtract, st);
   const Dims d = dims_of(c);
   const float scale = (float)(1.0 / (double)c->nvox);

@@ -230,6 +230,227 @@ __global__ void __launch_bounds__(kThreads, 1)
   cluster.sync();
 }
 
+// ---- prefetching variants ----------------------------------------------------
+// Shared-memory slabs arrive by cp.async while the previous coil or plane is
+// being transformed, so the global latency of a CTA's inputs is paid once.
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// dst[r·len + e] = src[r·gs + e], r < rows, e < len
+__device__ __forceinline__ void slab_async(cf* dst, const cf* src, int rows, int len, int64_t gs) {
+  const int tot = rows * len;
+  for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+    const int r = i / len, e = i - r * len;
+    cp_async8(dst + i, src + r * gs + e);
+  }
+}
+// dst[i] = src[i], i < cnt (16-byte copies when both ends allow it)
+__device__ __forceinline__ void span_async(cf* dst, const cf* src, int cnt) {
+  const bool v16 = ((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15) == 0;
+  if (v16) {
+    const int h = cnt >> 1;
+    for (int i = threadIdx.x; i < h; i += blockDim.x) cp_async16(dst + 2 * i, src + 2 * i);
+    if ((cnt & 1) && threadIdx.x == 0) cp_async8(dst + cnt - 1, src + cnt - 1);
+  } else {
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) cp_async8(dst + i, src + i);
+  }
+}
+
+struct ZLoadMulS {   // xs[z][x] · S'_c[z][x], both staged in shared memory
+  const cf* xs;
+  const cf* sc;
+  int Nx;
+  __device__ __forceinline__ cf operator()(int l, int e) const {
+    return cmul(xs[e * Nx + l], sc[e * Nx + l]);
+  }
+};
+struct ZAccS {       // acc[z][x] += conj(S'_c[z][x]) · v, S'_c staged in shared memory
+  cf* acc;
+  const cf* sc;
+  int Nx;
+  __device__ __forceinline__ void operator()(int l, int e, cf v) const {
+    cf& a = acc[e * Nx + l];
+    a = cadd(a, cmulc(sc[e * Nx + l], v));
+  }
+};
+
+// k_zfwd_fast with the coil-map slab of the next coil prefetched.
+// Shared: tw[Nz], xs, sc, A (, B for three-pass plans), each Nz·Nx.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_zfwd_pre(const cf* __restrict__ X, int ns, int64_t sstride, int t0,
+               const cf* __restrict__ smod, cf* __restrict__ T, Dims d, FPlan pz,
+               const cf* __restrict__ twz, int cpg) {
+  extern __shared__ __align__(16) cf sm[];
+  const int S = d.Nz * d.Nx;
+  cf* tw = sm;
+  cf* xs = tw + ((d.Nz + 1) & ~1);
+  cf* sc = xs + S;
+  cf* A = sc + S;
+  cf* B = A + S;
+  const int grp = blockIdx.x, y = blockIdx.y, f = blockIdx.z;
+  const int t = t0 + f;
+  const int64_t plane = (int64_t)d.Nx * d.Ny;
+  const int64_t ybase = (int64_t)y * d.Nx;
+  const int c0 = grp * cpg, c1 = min(d.Nc, c0 + cpg);
+  if (c0 < c1) slab_async(sc, smod + (int64_t)c0 * d.nvox + ybase, d.Nz, d.Nx, plane);
+  cp_commit();
+  load_tw(tw, twz, d.Nz);
+  for (int i = threadIdx.x; i < S; i += blockDim.x) {
+    const int z = i / d.Nx, x = i - z * d.Nx;
+    const int64_t off = (int64_t)t * d.nvox + z * plane + ybase + x;
+    cf v = X[off];
+    for (int k = 1; k < ns; ++k) v = cadd(v, X[off + k * sstride]);
+    xs[i] = v;
+  }
+  const Sm sa{A, 1, d.Nx}, sb{B, 1, d.Nx};
+  const ZLoadMulS ldf{xs, sc, d.Nx};
+  for (int c = c0; c < c1; ++c) {
+    cp_wait_all();
+    __syncthreads();
+    const Gm stl{T + ((int64_t)f * d.Nc + c) * d.nvox + ybase, 1, plane};
+    if (pz.npass == 1) {
+      fast::pass<false>(pz.fw[0], d.Nx, pz.Mnl, true, tw, ldf, stl);
+    } else {
+      fast::pass<false>(pz.fw[0], d.Nx, pz.Mnl, true, tw, ldf, sa);
+    }
+    if (c + 1 < c1) slab_async(sc, smod + (int64_t)(c + 1) * d.nvox + ybase, d.Nz, d.Nx, plane);
+    cp_commit();
+    if (pz.npass > 1)
+      run_passes<false>(pz.fw, 1, pz.npass, d.Nx, pz.Mnl, true, tw, sa, stl, false, true, sa, sb);
+  }
+}
+
+// k_zadj_fast with the next coil's k-space slab and coil-map slab prefetched.
+// Shared: tw[Nz], acc, A, P, SC0, SC1 (, B for three-pass plans), each Nz·Nx.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_zadj_pre(const cf* __restrict__ T, const cf* __restrict__ smod, cf* __restrict__ out,
+               const cf* __restrict__ ahy, int t0, float scale, int subtract, Dims d, FPlan pz,
+               const cf* __restrict__ twz, int cpg) {
+  extern __shared__ __align__(16) cf sm[];
+  const int S = d.Nz * d.Nx;
+  cf* tw = sm;
+  cf* acc = tw + ((d.Nz + 1) & ~1);
+  cf* A = acc + S;
+  cf* P = A + S;
+  cf* SC0 = P + S;
+  cf* SC1 = SC0 + S;
+  cf* B = SC1 + S;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int G = (int)cluster.num_blocks();
+  const int grp = (int)cluster.block_rank();
+  const int y = blockIdx.y, f = blockIdx.z;
+  const int t = t0 + f;
+  const int64_t plane = (int64_t)d.Nx * d.Ny;
+  const int64_t ybase = (int64_t)y * d.Nx;
+  const int c0 = grp * cpg, c1 = min(d.Nc, c0 + cpg);
+  auto tslab = [&](int c) { return T + ((int64_t)f * d.Nc + c) * d.nvox + ybase; };
+  if (c0 < c1) {
+    slab_async(P, tslab(c0), d.Nz, d.Nx, plane);
+    slab_async(SC0, smod + (int64_t)c0 * d.nvox + ybase, d.Nz, d.Nx, plane);
+  }
+  cp_commit();
+  load_tw(tw, twz, d.Nz);
+  for (int i = threadIdx.x; i < S; i += blockDim.x) acc[i] = make_float2(0.f, 0.f);
+  const Sm sa{A, 1, d.Nx}, sb{B, 1, d.Nx}, sp{P, 1, d.Nx};
+  for (int c = c0; c < c1; ++c) {
+    cp_wait_all();
+    __syncthreads();
+    const int q = c - c0;
+    // each output position is owned by one thread for every coil: no race on acc
+    const ZAccS stl{acc, (q & 1) ? SC1 : SC0, d.Nx};
+    if (pz.npass == 1) {
+      fast::pass<true>(pz.iv[0], d.Nx, pz.Mnl, true, tw, sp, stl);
+    } else {
+      fast::pass<true>(pz.iv[0], d.Nx, pz.Mnl, true, tw, sp, sa);
+    }
+    if (c + 1 < c1) {
+      slab_async(P, tslab(c + 1), d.Nz, d.Nx, plane);
+      slab_async((q & 1) ? SC0 : SC1, smod + (int64_t)(c + 1) * d.nvox + ybase, d.Nz, d.Nx, plane);
+    }
+    cp_commit();
+    if (pz.npass > 1)
+      run_passes<true>(pz.iv, 1, pz.npass, d.Nx, pz.Mnl, true, tw, sa, stl, false, true, sa, sb);
+  }
+  cluster.sync();
+  // rank g reduces positions [g·per, (g+1)·per) over ranks 0..G-1 in order
+  const int per = (S + G - 1) / G;
+  const int i0 = grp * per, i1 = min(S, i0 + per);
+  for (int i = i0 + (int)threadIdx.x; i < i1; i += blockDim.x) {
+    cf s = *cluster.map_shared_rank(acc + i, 0);
+    for (int q = 1; q < G; ++q) s = cadd(s, *cluster.map_shared_rank(acc + i, q));
+    const int z = i / d.Nx, x = i - z * d.Nx;
+    const int64_t off = (int64_t)t * d.nvox + z * plane + ybase + x;
+    cf v = cscale(s, scale);
+    if (subtract) v = csub(v, ahy[off]);
+    out[off] = v;
+  }
+  cluster.sync();
+}
+
+// Persistent normal-mode plane kernel: CTA b takes planes b, b + grid, ...
+// (plane u = kz + Nz·(c + Nc·f)); the next plane is copied into P while the
+// current one is transformed in A / B.  Shared: twx, twy, P, A, B.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_xy_pers(cf* __restrict__ T, const uint32_t* __restrict__ mask, int nwords, int t0, int nf,
+              Dims d, FPlan px, FPlan py, const cf* __restrict__ twx_g,
+              const cf* __restrict__ twy_g) {
+  extern __shared__ __align__(16) cf sm[];
+  const int Pl = d.Nx * d.Ny;
+  const int Nx = d.Nx, Ny = d.Ny;
+  cf* twx = sm;
+  cf* twy = twx + Nx;
+  cf* P = twy + ((Ny + 1) & ~1) + (Nx & 1);   // 16-byte aligned when sm is
+  cf* A = P + ((Pl + 1) & ~1);
+  cf* B = A + ((Pl + 1) & ~1);
+  const int units = d.Nz * d.Nc * nf;
+  auto plane_of = [&](int u) {
+    const int kz = u % d.Nz, r = u / d.Nz;
+    const int c = r % d.Nc, ff = r / d.Nc;
+    return T + ((int64_t)ff * d.Nc + c) * d.nvox + (int64_t)kz * Pl;
+  };
+  int u = blockIdx.x;
+  if (u < units) span_async(P, plane_of(u), Pl);
+  cp_commit();
+  load_tw(twx, twx_g, Nx);
+  load_tw(twy, twy_g, Ny);
+  auto rows = [&](cf* b) { return Sm{b, Nx, 1}; };
+  auto cols = [&](cf* b) { return Sm{b, 1, Nx}; };
+  auto other = [&](const cf* b) { return b == A ? B : A; };
+  for (; u < units; u += gridDim.x) {
+    cp_wait_all();
+    __syncthreads();
+    const int kz = u % d.Nz, ff = u / (d.Nz * d.Nc);
+    cf* pl = plane_of(u);
+    const Gm grow{pl, Nx, 1};
+    fast::pass<false>(px.fw[0], Ny, px.Mnl, false, twx, rows(P), rows(A));
+    const int nxt = u + (int)gridDim.x;
+    if (nxt < units) span_async(P, plane_of(nxt), Pl);
+    cp_commit();
+    Sm cur = run_passes<false>(px.fw, 1, px.npass, Ny, px.Mnl, false, twx, grow, grow, false,
+                               false, rows(A), rows(B));
+    cur = run_passes<false>(py.fw, 0, py.npass - 1, Nx, py.Mnl, true, twy, grow, grow, false,
+                            false, cols(cur.b), cols(other(cur.b)));
+    const Sm dst = cols(other(cur.b));
+    const MaskFn msk{mask + (int64_t)(t0 + ff) * nwords, (int64_t)kz * Pl, Nx};
+    fast::sandwich(py.fw[py.npass - 1], Nx, py.Mnl, true, twy, cols(cur.b), dst, msk);
+    cur = run_passes<true>(py.iv, 1, py.npass, Nx, py.Mnl, true, twy, grow, grow, false, false,
+                           dst, cols(other(dst.b)));
+    run_passes<true>(px.iv, 0, px.npass, Ny, px.Mnl, false, twx, grow, grow, false, true,
+                     rows(cur.b), rows(other(cur.b)));
+  }
+}
+
 // y[t][c][i] = s·φ(idx)·T[f][c][idx]  /  its adjoint scatter
 __device__ __forceinline__ cf phase_at(int64_t k, const cf* px, const cf* py, const cf* pz,
                                        const Dims& d) {
@@ -285,6 +506,18 @@ size_t smem_z(const Ctx* c, int npass) {
 }
 size_t smem_xy(const Ctx* c) {
   return sizeof(cf) * (c->N[0] + c->N[1] + 2 * (size_t)c->N[0] * c->N[1]);
+}
+size_t smem_zfwd_pre(const Ctx* c, int npass) {
+  const size_t S = (size_t)c->N[2] * c->N[0];
+  return sizeof(cf) * (((c->N[2] + 1) & ~1) + (npass >= 3 ? 4 : 3) * S);
+}
+size_t smem_zadj_pre(const Ctx* c, int npass) {
+  const size_t S = (size_t)c->N[2] * c->N[0];
+  return sizeof(cf) * (((c->N[2] + 1) & ~1) + (npass >= 3 ? 6 : 5) * S);
+}
+size_t smem_xy_pers(const Ctx* c) {
+  const size_t Pl = (size_t)c->N[0] * c->N[1];
+  return sizeof(cf) * (c->N[0] + ((c->N[1] + 1) & ~1) + (c->N[0] & 1) + 3 * ((Pl + 1) & ~1));
 }
 
 // Radices (1-3 passes, every radix in the menu, at most kThreads butterflies
@@ -352,6 +585,19 @@ bool sense_fast_setup(Ctx* c) {
     cudaGetLastError();
     return false;
   }
+  // prefetching variants where their extra buffers fit
+  constexpr size_t kMaxSmem = 227 * 1024;
+  const size_t szf = smem_zfwd_pre(c, np[2]), sza = smem_zadj_pre(c, np[2]), sxp = smem_xy_pers(c);
+  c->zpre = szf <= kMaxSmem && sza <= kMaxSmem &&
+            !cudaFuncSetAttribute(k_zfwd_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)szf) &&
+            !cudaFuncSetAttribute(k_zadj_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sza);
+  c->xypers = sxp <= kMaxSmem &&
+              !cudaFuncSetAttribute(k_xy_pers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sxp);
+  cudaGetLastError();
+  int dev = 0, nsm = 0;
+  if (!cudaGetDevice(&dev) && !cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) && nsm > 0)
+    c->nsm = nsm;
+  cudaGetLastError();
   return true;
 }
 
@@ -375,8 +621,14 @@ int launch_zadj(Ctx* c, const Dims& d, int G, int f, int t0, cf* out, const cf* 
   cfg.numAttrs = 1;
   const cf* T = c->d_T;
   const cf* smod = c->d_smaps_mod;
-  MSLR_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_zadj_fast, T, smod, out, ahy, t0, scale, subtract, d,
-                                   fp[2], (const cf*)c->d_tw[2], cpg));
+  if (c->zpre) {
+    cfg.dynamicSmemBytes = smem_zadj_pre(c, fp[2].npass);
+    MSLR_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_zadj_pre, T, smod, out, ahy, t0, scale, subtract, d,
+                                     fp[2], (const cf*)c->d_tw[2], cpg));
+  } else {
+    MSLR_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_zadj_fast, T, smod, out, ahy, t0, scale, subtract, d,
+                                     fp[2], (const cf*)c->d_tw[2], cpg));
+  }
   return MSLR_OK;
 }
 
@@ -391,10 +643,20 @@ int normal_op_fast(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
   const int cpg = (c->Nc + G - 1) / G;
   for (int t0 = 0; t0 < c->Nt; t0 += c->Ffast) {
     const int f = std::min(c->Ffast, c->Nt - t0);
-    k_zfwd_fast<<<dim3(G, d.Ny, f), kThreads, smem_z(c, fp[2].npass), st>>>(
-        X, ns, sstride, t0, c->d_smaps_mod, c->d_T, d, fp[2], c->d_tw[2], cpg);
-    k_xy_fast<<<dim3(d.Nz, d.Nc, f), kThreads, smem_xy(c), st>>>(
-        c->d_T, c->d_mask, c->nwords, t0, d, fp[0], fp[1], c->d_tw[0], c->d_tw[1], XY_NORMAL);
+    if (c->zpre)
+      k_zfwd_pre<<<dim3(G, d.Ny, f), kThreads, smem_zfwd_pre(c, fp[2].npass), st>>>(
+          X, ns, sstride, t0, c->d_smaps_mod, c->d_T, d, fp[2], c->d_tw[2], cpg);
+    else
+      k_zfwd_fast<<<dim3(G, d.Ny, f), kThreads, smem_z(c, fp[2].npass), st>>>(
+          X, ns, sstride, t0, c->d_smaps_mod, c->d_T, d, fp[2], c->d_tw[2], cpg);
+    if (c->xypers) {
+      const int units = d.Nz * d.Nc * f;
+      k_xy_pers<<<std::min(units, c->nsm), kThreads, smem_xy_pers(c), st>>>(
+          c->d_T, c->d_mask, c->nwords, t0, f, d, fp[0], fp[1], c->d_tw[0], c->d_tw[1]);
+    } else {
+      k_xy_fast<<<dim3(d.Nz, d.Nc, f), kThreads, smem_xy(c), st>>>(
+          c->d_T, c->d_mask, c->nwords, t0, d, fp[0], fp[1], c->d_tw[0], c->d_tw[1], XY_NORMAL);
+    }
     int rc = launch_zadj(c, d, G, f, t0, g, c->d_ahy, scale, subtract ? 1 : 0, st);
     if (rc) return rc;
     c->launches += 3;

@@ -1,0 +1,498 @@
+// sense_spec.cu — shape-specialised tuned SENSE normal operator.
+//
+// Same decomposition as sense_fast.cu (z pass | xy pass with the k-space mask
+// | z pass with the coil combine; the centring identity is in the header of
+// sense.cu), compiled for the image shapes listed at the bottom of this file
+// so that every axis plan, stride and line count is a compile-time constant
+// (fft_spec.cuh).  The work is ordered coil group by coil group (six coils),
+// two frames per chunk, so that a group's coil maps (6 × 3.9 MB at 90×90×60)
+// and the chunk's k-space T (2 × 6 × 3.9 MB) stay resident in L2 together;
+// the gradient g accumulates over the groups.  Per chunk:
+//   k_zfwd4  persistent       Σ_k X_k · S'_c → DFT_z → T, unit (cc, f, y);
+//                             coil-map slabs arrive by TMA three units ahead
+//   k_xy3    persistent       plane u: DFT_x, DFT_y, mask, bDFT_y, bDFT_x;
+//                             plane u + grid copied in while u is transformed
+//   k_zadj5  (ch, Ny, F),     bDFT_z → × conj(S'_c), one coil per CTA, two
+//            ch-CTA clusters  CTAs per SM; the cluster sums its coils through
+//                             distributed shared memory in rank order
+// Lines are owned by warps, so the passes of one axis need only __syncwarp;
+// block barriers separate the axes and guard the copy buffers.  Every wait on
+// an mbarrier is bounded: on time-out the thread stops computing, keeps
+// taking part in the barriers, and the CTA raises bit 8 of the device error
+// word (reported by the host after the POGM run).
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "fft_spec.cuh"
+#include "internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace mslr {
+
+namespace {
+
+using spec::Ax2;
+using spec::GmC;
+using spec::SmC;
+
+constexpr int kErrWait = 8;
+
+// A copy of p the compiler cannot see through: loads through it are not
+// hoisted out of the surrounding loop (which would pin every twiddle of every
+// pass in registers for the whole kernel).
+template <class T>
+__device__ __forceinline__ T* opaque(T* p) {
+  asm volatile("" : "+l"(p));
+  return p;
+}
+
+template <int NX_, int NY_, int NZ_, class AX_, class AY_, class AZ_>
+struct Shape {
+  static constexpr int NX = NX_, NY = NY_, NZ = NZ_;
+  using AX = AX_;
+  using AY = AY_;
+  using AZ = AZ_;
+  static_assert(AX::N == NX && AY::N == NY && AZ::N == NZ, "axis plans");
+  static_assert(NX % 2 == 0, "rows must be whole 16-byte units for the bulk copies");
+  static constexpr int PL = NX * NY;            // plane
+  static constexpr int S = NZ * NX;             // z slab (fixed y)
+  static constexpr int64_t NVOX = (int64_t)PL * NZ;
+  static constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
+  static constexpr int mn(int a, int b) { return a < b ? a : b; }
+  static constexpr int mx(int a, int b) { return a > b ? a : b; }
+  static constexpr int ZW = mn(32, cdiv(NX, AZ::LPW));                               // warps, z kernels
+  // warps of the plane kernel: at most 16, so that a thread may hold 128 registers
+  static constexpr int XYW = mn(16, mx(cdiv(NY, AX::LPW), cdiv(NX, AY::LPW)));
+  static constexpr int MW = (PL / 32 + 2 + 3) & ~3;   // mask words spanning one plane
+  static constexpr int ev(int n) { return (n + 1) & ~1; }
+  // warps of the adjoint z kernel (two CTAs per SM): at most 16
+  static constexpr int ZW2 = mn(16, cdiv(NX, AZ::LPW));
+  static constexpr size_t smem_zfwd = sizeof(cf) * (4 * (size_t)S + ev(NZ)) + 3 * sizeof(uint64_t);
+  static constexpr size_t smem_zadj = sizeof(cf) * (2 * (size_t)S + ev(NZ)) + sizeof(uint64_t);
+  static constexpr size_t smem_xy =
+      sizeof(cf) * (2 * (size_t)PL + ev(NX) + ev(NY)) + MW * sizeof(uint32_t) + sizeof(uint64_t);
+};
+
+// xs[z][x] · S'_c[z][x], both in shared memory (line = x, element = z)
+template <int NX>
+struct ZLd {
+  const cf* xs;
+  const cf* sc;
+  __device__ __forceinline__ cf operator()(int l, int e) const {
+    return cmul(xs[e * NX + l], sc[e * NX + l]);
+  }
+};
+// dst[z][x] = conj(S'_c[z][x]) · v (in place over the k-space slab)
+template <int NX>
+struct ZMulC {
+  cf* dst;
+  const cf* sc;
+  __device__ __forceinline__ void operator()(int l, int e, cf v) const {
+    dst[e * NX + l] = cmulc(sc[e * NX + l], v);
+  }
+};
+// k-space mask of one plane (line = kx, element = ky), bits staged in shared memory
+template <int NX>
+struct MaskS {
+  const uint32_t* w;
+  int off;   // bit index of (kx, ky) = (0, 0) within w
+  __device__ __forceinline__ cf operator()(int l, int e, cf v) const {
+    const int b = off + e * NX + l;
+    return ((w[b >> 5] >> (b & 31)) & 1u) ? v : make_float2(0.f, 0.f);
+  }
+};
+
+// Warp 0 copies `rows` rows of `len` complex values (row stride gs in global
+// memory, dense in shared memory) and arms `bar` for the bytes.
+__device__ __forceinline__ void rows_g2s(cf* dst, const cf* src, int rows, int len, int64_t gs,
+                                         uint64_t* bar) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    spec::fence_proxy_async();
+    spec::mbar_expect_tx(bar, (unsigned)(rows * len * sizeof(cf)));
+  }
+  __syncwarp();
+  for (int r = lane; r < rows; r += 32)
+    spec::bulk_g2s(dst + r * len, src + r * gs, (unsigned)(len * sizeof(cf)), bar);
+}
+
+// ---------------------------------------------------------------------------
+// Forward z pass of one coil group, persistent: unit u = (coil cc fastest,
+// then frame, then y slab); CTA b takes the contiguous units
+// [b·U/grid, (b+1)·U/grid), so the summed image slab Σ_k X_k is reloaded only
+// when (y, frame) changes.  S'_c slabs arrive three units ahead by TMA; both
+// passes run in place in the slab buffer; the result goes to T[f][cc][z][y][x].
+template <class Sh>
+__global__ void __launch_bounds__(Sh::ZW * 32, 1)
+    k_zfwd4(const cf* __restrict__ X, int ns, int64_t sstride, int t0, int nf, int cc0, int ch,
+            const cf* __restrict__ smod, cf* __restrict__ T, const cf* __restrict__ twz,
+            int* __restrict__ err) {
+  using AZ = typename Sh::AZ;
+  constexpr int NX = Sh::NX, NY = Sh::NY, NZ = Sh::NZ, S = Sh::S;
+  constexpr int64_t PLANE = Sh::PL, NVOX = Sh::NVOX;
+  constexpr int NB = 3;
+  static_assert(Sh::cdiv(NX, AZ::LPW) <= Sh::ZW, "one line group per warp");
+  extern __shared__ __align__(128) unsigned char smraw[];
+  cf* xs = reinterpret_cast<cf*>(smraw);
+  cf* scb0 = xs + S;   // NB slab buffers
+  cf* tw = scb0 + NB * S;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + Sh::ev(NZ));
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int U = NY * nf * ch;
+  const int u0 = (int)((int64_t)blockIdx.x * U / gridDim.x);
+  const int u1 = (int)((int64_t)(blockIdx.x + 1) * U / gridDim.x);
+  if (tid == 0) {
+    for (int i = 0; i < NB; ++i) spec::mbar_init(&bar[i], 1);
+    spec::mbar_fence_init();
+  }
+  __syncthreads();
+  auto issue = [&](int u, int b) {
+    const int cc = u % ch, y = (u / ch) / nf;
+    rows_g2s(scb0 + b * S, smod + (int64_t)(cc0 + cc) * NVOX + (int64_t)y * NX, NZ, NX, PLANE,
+             &bar[b]);
+  };
+  if (warp == 0)
+    for (int q = 0; q < NB && u0 + q < u1; ++q) issue(u0 + q, q);
+  for (int i = tid; i < NZ; i += blockDim.x) tw[i] = twz[i];
+  bool bad = false;
+  int cur = -1;
+  const int l0 = warp * AZ::LPW;
+  for (int u = u0; u < u1; ++u) {
+    const int q = u - u0, b = q % NB;
+    const int cc = u % ch, r = u / ch, ff = r % nf, y = r / nf;
+    if (r != cur) {   // new (y, frame): stage Σ_k X_k of the slab
+      const int64_t base = (int64_t)(t0 + ff) * NVOX + (int64_t)y * NX;
+      for (int i = tid; i < S; i += blockDim.x) {
+        const int z = i / NX, x = i - z * NX;
+        const int64_t off = base + z * PLANE + x;
+        cf v = X[off];
+        for (int k = 1; k < ns; ++k) v = cadd(v, X[off + k * sstride]);
+        xs[i] = v;
+      }
+      cur = r;
+      __syncthreads();
+    }
+    if (!bad && !spec::mbar_wait(&bar[b], (unsigned)((q / NB) & 1))) bad = true;
+    if (!bad && l0 < NX) {
+      cf* sc = scb0 + b * S;
+      cf* Tc = T + ((int64_t)ff * ch + cc) * NVOX + (int64_t)y * NX;
+      const cf* twc = opaque(tw);
+      spec::wpass<NZ, AZ::R0, 1, false, AZ::LPW, true>(l0, NX, twc, ZLd<NX>{xs, sc},
+                                                       SmC<1, NX>{sc});
+      spec::wpass<NZ, AZ::R1, AZ::R0, false, AZ::LPW, false>(l0, NX, twc, SmC<1, NX>{sc},
+                                                             GmC<1>{Tc, PLANE});
+    }
+    __syncthreads();   // slab buffer b and xs are free
+    if (warp == 0 && q + NB < u1 - u0) issue(u + NB, b);
+  }
+  if (__syncthreads_or(bad) && tid == 0) atomicOr(err, kErrWait);
+}
+
+// The three phases of a plane, each over the lines of group l0.  Kept out of
+// line so that one phase's index arithmetic is not hoisted into the plane
+// loop next to the others' (which overflows the 64-register budget).
+template <class Sh>
+__device__ __noinline__ void xy_rows_fwd(const cf* P, cf* A, const cf* twx, int l0) {
+  using AX = typename Sh::AX;
+  using Rows = SmC<Sh::NX, 1>;
+  spec::wpass<Sh::NX, AX::R0, 1, false, AX::LPW, false>(l0, Sh::NY, twx, Rows{const_cast<cf*>(P)},
+                                                        Rows{A});
+  spec::wpass<Sh::NX, AX::R1, AX::R0, false, AX::LPW, true>(l0, Sh::NY, twx, Rows{A}, Rows{A});
+}
+template <class Sh>
+__device__ __noinline__ void xy_cols(cf* A, const cf* twy, int l0, const uint32_t* smask, int moff) {
+  using AY = typename Sh::AY;
+  using Cols = SmC<1, Sh::NX>;
+  const MaskS<Sh::NX> msk{smask, moff};
+  spec::wpass<Sh::NY, AY::R0, 1, false, AY::LPW, true>(l0, Sh::NX, twy, Cols{A}, Cols{A});
+  spec::wsandwich<Sh::NY, AY::R1, AY::LPW, true>(l0, Sh::NX, twy, Cols{A}, Cols{A}, msk);
+  spec::wpass<Sh::NY, AY::R0, AY::R1, true, AY::LPW, true>(l0, Sh::NX, twy, Cols{A}, Cols{A});
+}
+template <class Sh>
+__device__ __noinline__ void xy_rows_inv(cf* A, const cf* twx, int l0, cf* pl) {
+  using AX = typename Sh::AX;
+  using Rows = SmC<Sh::NX, 1>;
+  spec::wpass<Sh::NX, AX::R1, 1, true, AX::LPW, true>(l0, Sh::NY, twx, Rows{A}, Rows{A});
+  spec::wpass<Sh::NX, AX::R0, AX::R1, true, AX::LPW, false>(l0, Sh::NY, twx, Rows{A}, Rows{pl});
+}
+
+// ---------------------------------------------------------------------------
+template <class Sh>
+__global__ void __launch_bounds__(Sh::XYW * 32, 1)
+    k_xy3(cf* __restrict__ T, const uint32_t* __restrict__ mask, int nwords, int t0, int nf,
+          int Nc, const cf* __restrict__ twx_g, const cf* __restrict__ twy_g,
+          int* __restrict__ err) {
+  using AX = typename Sh::AX;
+  using AY = typename Sh::AY;
+  constexpr int NX = Sh::NX, NY = Sh::NY, NZ = Sh::NZ, PL = Sh::PL, MW = Sh::MW;
+  constexpr int64_t NVOX = Sh::NVOX;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  cf* P = reinterpret_cast<cf*>(smraw);
+  cf* A = P + PL;
+  cf* twx = A + PL;
+  cf* twy = twx + Sh::ev(NX);
+  uint32_t* smask = reinterpret_cast<uint32_t*>(twy + Sh::ev(NY));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smask + MW);
+  const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int units = NZ * Nc * nf;
+  auto plane_of = [&](int u) {
+    const int kz = u % NZ, r = u / NZ;
+    const int c = r % Nc, ff = r / Nc;
+    return T + ((int64_t)ff * Nc + c) * NVOX + (int64_t)kz * PL;
+  };
+  if (tid == 0) {
+    spec::mbar_init(bar, 1);
+    spec::mbar_fence_init();
+  }
+  for (int i = tid; i < NX; i += blockDim.x) twx[i] = twx_g[i];
+  for (int i = tid; i < NY; i += blockDim.x) twy[i] = twy_g[i];
+  __syncthreads();
+  int u = blockIdx.x;
+  if (tid == 0 && u < units) {
+    spec::mbar_expect_tx(bar, PL * (unsigned)sizeof(cf));
+    spec::bulk_g2s(P, plane_of(u), PL * (unsigned)sizeof(cf), bar);
+  }
+  unsigned par = 0;
+  bool bad = false;
+  for (; u < units; u += gridDim.x) {
+    const int kz = u % NZ, ff = u / (NZ * Nc);
+    const int64_t bit0 = (int64_t)kz * PL;
+    const int w0 = (int)(bit0 >> 5);
+    const uint32_t* mrow = mask + (int64_t)(t0 + ff) * nwords;
+    for (int i = tid; i < MW; i += blockDim.x) smask[i] = (w0 + i < nwords) ? __ldg(mrow + w0 + i) : 0u;
+    if (!bad && !spec::mbar_wait(bar, par)) bad = true;
+    par ^= 1u;
+    if (!bad) {
+#pragma unroll 1
+      for (int g = warp; g * AX::LPW < NY; g += nw) xy_rows_fwd<Sh>(P, A, twx, g * AX::LPW);
+    }
+    __syncthreads();   // rows done; P free; mask words visible
+    const int nxt = u + (int)gridDim.x;
+    if (tid == 0 && nxt < units) {
+      spec::fence_proxy_async();
+      spec::mbar_expect_tx(bar, PL * (unsigned)sizeof(cf));
+      spec::bulk_g2s(P, plane_of(nxt), PL * (unsigned)sizeof(cf), bar);
+    }
+    if (!bad) {
+      const int moff = (int)(bit0 - (int64_t)w0 * 32);
+#pragma unroll 1
+      for (int g = warp; g * AY::LPW < NX; g += nw) xy_cols<Sh>(A, twy, g * AY::LPW, smask, moff);
+    }
+    __syncthreads();   // columns done
+    if (!bad) {
+      cf* pl = plane_of(u);
+#pragma unroll 1
+      for (int g = warp; g * AX::LPW < NY; g += nw) xy_rows_inv<Sh>(A, twx, g * AX::LPW, pl);
+    }
+  }
+  if (__syncthreads_or(bad) && tid == 0) atomicOr(err, kErrWait);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint z pass of one coil group: CTA (cc, y, f) of a cluster of `ch` CTAs
+// (one per coil) takes the k-space slab of coil cc and its coil-map slab by
+// TMA, runs both inverse passes in place, multiplies by conj(S'_c), and the
+// cluster sums its coils through distributed shared memory in rank order into
+// out (mode 0: scale·Σ − A'y when subtract, mode 1: out += scale·Σ).
+template <class Sh>
+__global__ void __launch_bounds__(Sh::ZW2 * 32, 2)
+    k_zadj5(const cf* __restrict__ T, const cf* __restrict__ smod, cf* __restrict__ out,
+            const cf* __restrict__ ahy, int t0, int cc0, float scale, int mode, int subtract,
+            const cf* __restrict__ twz, int* __restrict__ err) {
+  using AZ = typename Sh::AZ;
+  constexpr int NX = Sh::NX, NZ = Sh::NZ, S = Sh::S;
+  constexpr int64_t PLANE = Sh::PL, NVOX = Sh::NVOX;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  cf* P = reinterpret_cast<cf*>(smraw);
+  cf* SC = P + S;
+  cf* tw = SC + S;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + Sh::ev(NZ));
+  cg::cluster_group cluster = cg::this_cluster();
+  const int G = (int)cluster.num_blocks();
+  const int cc = (int)cluster.block_rank();
+  const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int y = blockIdx.y, f = blockIdx.z;
+  const int t = t0 + f;
+  const int64_t ybase = (int64_t)y * NX;
+  if (tid == 0) {
+    spec::mbar_init(bar, 1);
+    spec::mbar_fence_init();
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int lane = tid & 31;
+    if (lane == 0) spec::mbar_expect_tx(bar, 2u * S * (unsigned)sizeof(cf));
+    __syncwarp();
+    const cf* ts = T + ((int64_t)f * G + cc) * NVOX + ybase;
+    const cf* ss = smod + (int64_t)(cc0 + cc) * NVOX + ybase;
+    for (int r = lane; r < NZ; r += 32) {
+      spec::bulk_g2s(P + r * NX, ts + r * PLANE, NX * (unsigned)sizeof(cf), bar);
+      spec::bulk_g2s(SC + r * NX, ss + r * PLANE, NX * (unsigned)sizeof(cf), bar);
+    }
+  }
+  for (int i = tid; i < NZ; i += blockDim.x) tw[i] = twz[i];
+  __syncthreads();
+  const bool bad = !spec::mbar_wait(bar, 0);
+  if (!bad) {
+    const cf* twc = opaque(tw);
+    using Cols = SmC<1, NX>;   // line = x, element = z
+#pragma unroll 1
+    for (int g = warp; g * AZ::LPW < NX; g += nw) {
+      spec::wpass<NZ, AZ::R1, 1, true, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
+      spec::wpass<NZ, AZ::R0, AZ::R1, true, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P},
+                                                           ZMulC<NX>{P, SC});
+    }
+  }
+  if (__syncthreads_or(bad) && tid == 0) atomicOr(err, kErrWait);
+  cluster.sync();
+  // rank g sums positions [g·per, (g+1)·per) over ranks 0..G-1 in order
+  const int per = (S + G - 1) / G;
+  const int i0 = cc * per, i1 = min(S, i0 + per);
+  for (int i = i0 + tid; i < i1; i += blockDim.x) {
+    cf s = *cluster.map_shared_rank(P + i, 0);
+    for (int q = 1; q < G; ++q) s = cadd(s, *cluster.map_shared_rank(P + i, q));
+    const int z = i / NX, x = i - z * NX;
+    const int64_t off = (int64_t)t * NVOX + z * PLANE + ybase + x;
+    cf v = cscale(s, scale);
+    if (mode) v = cadd(out[off], v);
+    else if (subtract) v = csub(v, ahy[off]);
+    out[off] = v;
+  }
+  cluster.sync();
+}
+
+// ---------------------------------------------------------------------------
+struct SpecOps {
+  int nx, ny, nz;
+  const void* zfwd;
+  const void* xy;
+  const void* zadj;
+  int zfwd_threads, xy_threads, zadj_threads;
+  size_t smem_zfwd, smem_zadj, smem_xy;
+};
+
+template <class Sh>
+SpecOps ops_of() {
+  return SpecOps{Sh::NX,
+                 Sh::NY,
+                 Sh::NZ,
+                 reinterpret_cast<const void*>(&k_zfwd4<Sh>),
+                 reinterpret_cast<const void*>(&k_xy3<Sh>),
+                 reinterpret_cast<const void*>(&k_zadj5<Sh>),
+                 Sh::ZW * 32,
+                 Sh::XYW * 32,
+                 Sh::ZW2 * 32,
+                 Sh::smem_zfwd,
+                 Sh::smem_zadj,
+                 Sh::smem_xy};
+}
+
+// Compiled shapes: the reference's fMRI volume (90×90×60) and smaller cubes
+// used by its tests and synthetic studies.
+using S90 = Shape<90, 90, 60, Ax2<90, 10, 9>, Ax2<90, 10, 9>, Ax2<60, 10, 6>>;
+using S48 = Shape<48, 48, 32, Ax2<48, 8, 6>, Ax2<48, 8, 6>, Ax2<32, 8, 4>>;
+using S32 = Shape<32, 32, 24, Ax2<32, 8, 4>, Ax2<32, 8, 4>, Ax2<24, 6, 4>>;
+
+const SpecOps* find_ops(int nx, int ny, int nz) {
+  static const SpecOps table[] = {ops_of<S90>(), ops_of<S48>(), ops_of<S32>()};
+  for (const SpecOps& o : table)
+    if (o.nx == nx && o.ny == ny && o.nz == nz) return &o;
+  return nullptr;
+}
+
+}  // namespace
+
+bool sense_spec_setup(Ctx* c) {
+  const SpecOps* o = find_ops(c->N[0], c->N[1], c->N[2]);
+  if (!o) return false;
+  if (cudaFuncSetAttribute(o->zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zfwd) ||
+      cudaFuncSetAttribute(o->zadj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zadj) ||
+      cudaFuncSetAttribute(o->xy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_xy)) {
+    cudaGetLastError();
+    return false;
+  }
+  int per_sm = 0, per_sm_z = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, o->xy, o->xy_threads, o->smem_xy) ||
+      per_sm < 1 ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_z, o->zfwd, o->zfwd_threads,
+                                                    o->smem_zfwd) ||
+      per_sm_z < 1) {
+    cudaGetLastError();
+    return false;
+  }
+  int dev = 0, nsm = 0;
+  if (!cudaGetDevice(&dev) && !cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) &&
+      nsm > 0)
+    c->nsm = nsm;
+  cudaGetLastError();
+  c->spec_xy_ctas = per_sm * c->nsm;
+  c->spec_zfwd_ctas = per_sm_z * c->nsm;
+  return true;
+}
+
+int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
+                   cudaStream_t st) {
+  const SpecOps* o = find_ops(c->N[0], c->N[1], c->N[2]);
+  if (!o) return fail(MSLR_ERR_UNSUPPORTED, "no specialised SENSE kernels for this shape");
+  float scale = (float)(1.0 / (double)c->nvox);
+  const int Nc = c->Nc, Ny = c->N[1], Nz = c->N[2];
+  const int Ch = std::min(Nc, 6);                                  // coils per group
+  const int F = ((int64_t)c->F * Nc >= 2 * (int64_t)Ch) ? 2 : 1;   // frames per chunk
+  int nwords = c->nwords;
+  const cf* smod = c->d_smaps_mod;
+  const uint32_t* mask = c->d_mask;
+  const cf* ahy = c->d_ahy;
+  cf* T = c->d_T;
+  int* err = c->d_err;
+  int sub = subtract ? 1 : 0;
+  for (int cc0 = 0; cc0 < Nc; cc0 += Ch) {
+    int ch = std::min(Ch, Nc - cc0);
+    int mode = cc0 > 0 ? 1 : 0;
+    for (int t0 = 0; t0 < c->Nt; t0 += F) {
+      int f = std::min(F, c->Nt - t0);
+      {
+        const int U = Ny * f * ch;
+        const int grid = std::max(1, std::min(U, c->spec_zfwd_ctas));
+        void* args[] = {(void*)&X,  (void*)&ns,   (void*)&sstride, (void*)&t0,
+                        (void*)&f,  (void*)&cc0,  (void*)&ch,      (void*)&smod,
+                        (void*)&T,  (void*)&c->d_tw[2], (void*)&err};
+        MSLR_CUDA_TRY(cudaLaunchKernel(o->zfwd, dim3(grid), dim3(o->zfwd_threads), args,
+                                       o->smem_zfwd, st));
+      }
+      {
+        const int units = Nz * ch * f;
+        const int grid = std::max(1, std::min(units, c->spec_xy_ctas));
+        void* args[] = {(void*)&T,  (void*)&mask,       (void*)&nwords,      (void*)&t0, (void*)&f,
+                        (void*)&ch, (void*)&c->d_tw[0], (void*)&c->d_tw[1], (void*)&err};
+        MSLR_CUDA_TRY(
+            cudaLaunchKernel(o->xy, dim3(grid), dim3(o->xy_threads), args, o->smem_xy, st));
+      }
+      {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(ch, Ny, f);
+        cfg.blockDim = dim3(o->zadj_threads, 1, 1);
+        cfg.dynamicSmemBytes = o->smem_zadj;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = ch;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        const cf* Tc = T;
+        void* args[] = {(void*)&Tc,   (void*)&smod, (void*)&g,   (void*)&ahy,
+                        (void*)&t0,   (void*)&cc0,  (void*)&scale, (void*)&mode,
+                        (void*)&sub,  (void*)&c->d_tw[2], (void*)&err};
+        MSLR_CUDA_TRY(cudaLaunchKernelExC(&cfg, o->zadj, args));
+      }
+      c->launches += 3;
+    }
+  }
+  MSLR_CUDA_TRY(cudaGetLastError());
+  return MSLR_OK;
+}
+
+}  // namespace mslr

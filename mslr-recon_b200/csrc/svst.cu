@@ -333,7 +333,24 @@ int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w,
   return MSLR_OK;
 }
 
-// Gram → eig → (rebuild into out or pbuf) for all patches described by m.
+// W = Ṽ Ṽᴴ for every patch, from the eigen stage's Ṽ (stored conjugated,
+// row-major, in w.zv) into w.gram: the Gram of n × n matrices read as "tall"
+// batch patches, M[a][l] = conj(zv[a·n + l]) = Ṽ[a][l].
+int svst_form_w(const WorkPtrs& w, int n, int64_t np, bool tc, cudaStream_t st,
+                uint64_t* launches) {
+  PatchMap vm{};
+  vm.batch = 1;
+  vm.tall = 1;
+  vm.Nt = n;
+  vm.p = n;
+  vm.n = n;
+  vm.L = n;
+  vm.nvox = n;
+  vm.mstride = (int64_t)n * n;
+  return svst_gram(reinterpret_cast<const cf*>(w.zv), vm, np, w, 1, tc, st, launches);
+}
+
+// Gram → eig → W → (rebuild into out or pbuf) for all patches described by m.
 int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
               const double* thr, int thr_per_patch, double lam, cf* out, int direct, bool tc,
               cudaStream_t st, uint64_t* launches) {
@@ -343,6 +360,7 @@ int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
   rc = eig2_launch(m.n, np, w.gram, reinterpret_cast<cf*>(w.zv), reinterpret_cast<float*>(w.aux),
                    w.rank, thr, thr_per_patch, lam, st);
   if (rc) return rc;
+  if ((rc = svst_form_w(w, m.n, np, tc, st, launches))) return rc;
   return svst_rebuild(in, m, np, w, out, direct, tc, st, launches);
 }
 
@@ -542,6 +560,8 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
   }
   if ((rc = eig_launch_multi(c->Ns, segs.data(), thr_dev, 0, st))) return rc;
   c->launches += 1;
+  for (int k = 0; k < c->Ns; ++k)
+    if ((rc = svst_form_w(ws[k], c->scales[k].n, c->scales[k].Np, true, st, &c->launches))) return rc;
   for (int k = 0; k < c->Ns; ++k) {
     const ScaleGeom& g = c->scales[k];
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
