@@ -32,6 +32,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "metric"
+# DRAM bytes (read + write) of one plane-pass launch (2 frames × 6 coils × 60
+# planes), from the ncu capture summarised in profiles/sense_chunk_kernels_90x90x60.md
+# (cold cache: ncu flushes L2 before the launch, so this is an upper bound)
+PLANE_TRAFFIC_PER_LAUNCH = 47254016 + 2285056
+# B200 FP32 FMA peak: 148 SMs × 128 lanes × 2 flops × 1.965 GHz (nominal)
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 def load_problem(name: str, seed_offset: int = 0):
@@ -307,22 +313,38 @@ def main():
     phases = {"normal_op_ms": t_normal * 1e3, "svst_ms": [t * 1e3 for t in t_svst]}
     if args.phases:
         log("phases", json.dumps(phases))
-    # roofline of the dominant phase (HBM-bound: algorithmic bytes / time)
+    # roofline of the dominant kernel: the plane pass of the SENSE normal operator
+    # (per-launch device time from events around every launch of one normal op)
     from mslr_recon_b200 import roofline as RL
     peaks = RL.peaks()
     Ns = len(pb["patch_sizes"])
-    dom = "normal_op" if t_normal >= max(t_svst) else f"svst_scale{int(np.argmax(t_svst))}"
-    if dom == "normal_op":
-        byts = RL.normal_op_bytes(nvox, Nt, Nc, Ns)
-        tdom = t_normal
+    roof = None
+    try:
+        kms, nl = ctx.normal_profile(X, out=g)
+    except Exception as exc:   # shapes without the specialised kernels
+        kms, nl = None, 0
+        log("no per-kernel profile:", exc)
+    if kms:
+        phases["normal_op_kernel_ms"] = kms
+        phases["normal_op_launches_per_kernel"] = nl
+        planes_per_launch = Nz * min(Nc, 6) * 2   # a chunk: one coil group (6), two frames
+        byts = RL.plane_pass_bytes(Nx, Ny, planes_per_launch)
+        fl = RL.plane_pass_flops(Nx, Ny, planes_per_launch)
+        tdom = kms["xy"] / 1e3
+        achieved = byts / tdom / 1e9
+        roof = {"bound": "hbm", "kernel": "k_xy3 (plane pass: DFT_x, DFT_y, mask, inverse)",
+                "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": PLANE_TRAFFIC_PER_LAUNCH,
+                "algorithmic_bytes_per_launch": byts, "launch_ms": kms["xy"],
+                "peak_source": peaks["source"],
+                "fp32": {"achieved_tflops": fl / tdom / 1e12, "nominal_peak_tflops": FP32_NOMINAL_TFLOPS,
+                         "note": "FP32 SIMT FFT; nominal 5 N log2 N flops; peak is nominal, not measured"}}
     else:
-        k = int(np.argmax(t_svst))
-        byts = RL.svst_bytes(nvox, Nt)
-        tdom = t_svst[k]
-    achieved = byts / tdom / 1e9
-    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peaks["hbm_gbs"],
-            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
-            "algorithmic_bytes": byts, "peak_source": peaks["source"]}
+        byts = RL.normal_op_bytes(nvox, Nt, Nc, Ns)
+        achieved = byts / t_normal / 1e9
+        roof = {"bound": "hbm", "kernel": "normal_op", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "algorithmic_bytes": byts, "peak_source": peaks["source"]}
 
     plain_ips = None
     if not args.no_plain and args.form == "tuned":

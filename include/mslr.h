@@ -151,6 +151,16 @@ int mslr_sense_adjoint(mslr_ctx* ctx, const void* y, void* x, void* stream);
 int mslr_normal_op(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g,
                    int32_t subtract_data, void* stream);
 
+/* Profiling hook (no counterpart in the reference): runs mslr_normal_op with
+ * subtract_data = 1 once, recording CUDA events on `stream` around every
+ * kernel, and returns the average device time per launch of the three
+ * kernels of a chunk — kernel_ms[0] forward z pass, [1] plane (x, y, mask)
+ * pass, [2] adjoint z pass with the coil combine — and the launches of each.
+ * Synchronises `stream`.  MSLR_ERR_UNSUPPORTED unless the tuned form runs the
+ * shape-specialised SENSE kernels for this image shape. */
+int mslr_normal_op_profile(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g, void* stream,
+                           double* kernel_ms, int64_t* launches_per_kernel);
+
 /* patchSVST for scale `scale` (0-based) with global threshold beta
  * (src/recon.jl:251-256; src/sense_gpu.jl:138-145): img_in (Nx,Ny,Nz,Nt)
  * -> img_out.  img_in may equal img_out. */
@@ -176,6 +186,11 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
 int mslr_pogm_begin(mslr_ctx* ctx, void* X, int32_t niter, double L, double restart_cutoff,
                     double bsig, void* stream);
 int mslr_pogm_step(mslr_ctx* ctx, void* X, void* stream);
+
+/* Tuned form only: capture the POGM iteration into a CUDA graph on first use
+ * and replay it (enable = 1, the default), or launch its kernels directly
+ * (enable = 0).  Both give bit-identical results. */
+int mslr_set_graph(mslr_ctx* ctx, int32_t enable);
 /* Restart flags of the iterations run so far (host array of niter+1). */
 int mslr_pogm_restarts(mslr_ctx* ctx, uint8_t* restarts_host, void* stream);
 

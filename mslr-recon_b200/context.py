@@ -148,6 +148,27 @@ class MSLRContext:
                                      1 if subtract_data else 0, _stream_ptr(stream)))
         return g
 
+    def set_graph(self, enable: bool):
+        """Tuned form: replay the POGM iteration from a captured CUDA graph
+        (default) or launch its kernels directly."""
+        self._chk(lib.mslr_set_graph(self._h, 1 if enable else 0))
+
+    def normal_profile(self, X: torch.Tensor, out=None, stream=None):
+        """One normal operator with events around every kernel: returns
+        ({"zfwd": ms, "xy": ms, "zadj": ms} average per launch, launches of each)."""
+        import ctypes as C
+        if X.dim() == 4:
+            X = X.unsqueeze(0)
+        ns = X.shape[0]
+        _dev_c64(X, (ns,) + self.img_shape, "X")
+        g = out if out is not None else torch.empty(self.img_shape, dtype=torch.complex64,
+                                                    device=X.device)
+        ms = (C.c_double * 3)()
+        n = (C.c_int64 * 3)()
+        self._chk(lib.mslr_normal_op_profile(self._h, X.data_ptr(), ns, g.data_ptr(),
+                                             _stream_ptr(stream), ms, n))
+        return {"zfwd": ms[0], "xy": ms[1], "zadj": ms[2]}, int(n[0])
+
     def patch_svst(self, scale: int, beta: float, img: torch.Tensor, out=None, stream=None):
         _dev_c64(img, self.img_shape, "img")
         o = out if out is not None else torch.empty_like(img)

@@ -48,6 +48,11 @@ static void free_ctx(mslr_ctx* c) {
   for (auto& w : c->svw)
     if (w.gram) cudaFree(w.gram);
   for (auto& g : c->scales) geom_free(&g);
+  for (cudaEvent_t e : c->prof_ev) cudaEventDestroy(e);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->gev_in) cudaEventDestroy(c->gev_in);
+  if (c->gev_out) cudaEventDestroy(c->gev_out);
+  if (c->gstream) cudaStreamDestroy(c->gstream);
   delete c;
 }
 
@@ -259,6 +264,41 @@ int mslr_normal_op(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g, int32_t
   return MSLR_OK;
 }
 
+int mslr_normal_op_profile(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g, void* stream,
+                           double* kernel_ms, int64_t* launches_per_kernel) {
+  CTX_CHECK(ctx);
+  NEED_BOUND(ctx);
+  if (!X || !g || ns_in <= 0 || !kernel_ms || !launches_per_kernel)
+    return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad argument"));
+  if (!ctx->spec)
+    return ctx_fail(ctx, fail(MSLR_ERR_UNSUPPORTED,
+                              "launch profiling needs the shape-specialised SENSE kernels"));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  ctx->prof_on = true;
+  ctx->prof_n = 0;
+  const int rc = normal_op(ctx, reinterpret_cast<const cf*>(X), ns_in, (int64_t)ctx->Nt * ctx->nvox,
+                           reinterpret_cast<cf*>(g), true, st);
+  ctx->prof_on = false;
+  if (rc) return ctx_fail(ctx, rc);
+  if (ctx->prof_n % 4) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "profiling events out of step"));
+  cudaError_t e = cudaEventSynchronize(ctx->prof_ev[ctx->prof_n - 1]);
+  if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
+  double tot[3] = {0.0, 0.0, 0.0};
+  const int chunks = ctx->prof_n / 4;
+  for (int q = 0; q < chunks; ++q)
+    for (int k = 0; k < 3; ++k) {
+      float ms = 0.f;
+      e = cudaEventElapsedTime(&ms, ctx->prof_ev[4 * q + k], ctx->prof_ev[4 * q + k + 1]);
+      if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
+      tot[k] += ms;
+    }
+  for (int k = 0; k < 3; ++k) {
+    kernel_ms[k] = chunks ? tot[k] / chunks : 0.0;
+    launches_per_kernel[k] = chunks;
+  }
+  return MSLR_OK;
+}
+
 int mslr_patch_svst(mslr_ctx* ctx, int32_t scale, double beta, const void* img_in, void* img_out,
                     void* stream) {
   CTX_CHECK(ctx);
@@ -348,6 +388,12 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
     return ctx_fail(ctx, fail(MSLR_ERR_NONFINITE, "non-finite value in the POGM restart sums"));
   if (herr & 8)
     return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a device-side wait for a bulk copy timed out"));
+  return MSLR_OK;
+}
+
+int mslr_set_graph(mslr_ctx* ctx, int32_t enable) {
+  CTX_CHECK(ctx);
+  ctx->use_graph = enable != 0;
   return MSLR_OK;
 }
 

@@ -15,8 +15,10 @@
 //      the previous step's rank-2 update on the fly while forming the next
 //      Hermitian matrix-vector product over 32 × 32 tiles of the trailing
 //      lower triangle (one warp per tile: row sums per lane, column sums by a
-//      shuffle transpose-reduction), so the trailing triangle is streamed
-//      once per step and the working set of ~300 resident patches stays in L2.
+//      shuffle transpose-reduction, both stored per tile and summed per row
+//      in a fixed order, so results are bit-reproducible), streaming the
+//      trailing triangle once per step; the working set of ~300 resident
+//      patches stays in L2.
 //   2. Eigenvalues of T above β² by bisection on FP64 Sturm counts, one
 //      thread per eigenvalue.
 //   3. Eigenvectors of T by FP64 twisted factorisation, one thread per
@@ -107,12 +109,19 @@ struct EigArgs {
 };
 
 // vectors are padded to n + 32 entries (zero tails) so 32-wide tiles read them in bounds
-size_t smem_bytes(int n) {
+// Per-tile partial sums of the tridiagonalisation's matvec: 64 values for
+// each 32 × 32 tile of the largest trailing triangle (side n − 1).
+size_t part_bytes(int n) {
+  const size_t T = (size_t)(n - 1 + 31) / 32;
+  return T * (T + 1) / 2 * 64 * sizeof(cf);
+}
+
+size_t smem_bytes(int n, int threads) {
   const size_t np = (size_t)n + 32;
-  const size_t vecs = 4 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
+  const size_t vecs = 3 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
                       3 * (size_t)n * sizeof(float) + 64 * sizeof(float) + 64 * sizeof(double);
   const size_t wy = (size_t)n * kNb * sizeof(cf) + 2 * kNb * kNb * sizeof(cf);
-  return vecs + wy + 128;
+  return vecs + std::max(wy, threads <= kSmallT ? part_bytes(n) : (size_t)0) + 128;
 }
 
 template <int MAXT, int MINB>
@@ -139,8 +148,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   cf* sv = reinterpret_cast<cf*>(redd + 64);        // v of this step  [npad]
   cf* svp = sv + npad;                              // previous v      [npad]
   cf* swp = svp + npad;                             // previous w      [npad]
-  cf* ys = swp + npad;                              // y accumulator   [npad]
-  float* hv = reinterpret_cast<float*>(ys + npad);  // h               [n]
+  float* hv = reinterpret_cast<float*>(swp + npad); // h               [n]
   float* taur = hv + n;                             // τ               [n]
   float* taui = taur + n;                           //                 [n]
   float* red0 = taui + n;                           // 2 × 32 floats
@@ -159,11 +167,14 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     sv[q] = make_float2(0.f, 0.f);
     svp[q] = make_float2(0.f, 0.f);
     swp[q] = make_float2(0.f, 0.f);
-    ys[q] = make_float2(0.f, 0.f);
   }
   __syncthreads();
   const int i = tid;   // row owned by this thread (n <= kT)
   const int warp = tid >> 5, lane = tid & 31, nwarp = kT >> 5;
+  // per-tile row / column sums of the Hermitian matvec of a step: shared
+  // memory (sharing the WY blocks' storage) for the 384-thread variant, the
+  // patch's FP64 pivot scratch (idle until phase 3) for the large variant
+  cf* part = (MAXT <= kSmallT) ? sY : reinterpret_cast<cf*>(AUX);
   for (int k = 0; k < n - 1; ++k) {
     // current column k and diagonal k: stored − (vp wpᴴ + wp vpᴴ)
     cf x = make_float2(0.f, 0.f);
@@ -297,25 +308,30 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
           ci[0] += __shfl_xor_sync(0xffffffffu, ci[0], 2);
           cr[0] += __shfl_xor_sync(0xffffffffu, cr[0], 1);
           ci[0] += __shfl_xor_sync(0xffffffffu, ci[0], 1);
-          const int jc = jb + (lane >> 2);
-          if (jc < n) {
-            if ((lane & 3) == 0) atomicAdd(&ys[jc].x, cr[0]);
-            else if ((lane & 3) == 1) atomicAdd(&ys[jc].y, ci[0]);
-          }
+          if ((lane & 3) == 0 && jb + (lane >> 2) < n)
+            part[(2 * t + 1) * 32 + g8 * 8 + (lane >> 2)] = make_float2(cr[0], ci[0]);
         }
-        if (rowok) {
-          atomicAdd(&ys[row].x, yr);
-          atomicAdd(&ys[row].y, yim);
-        }
+        part[2 * t * 32 + lane] = make_float2(yr, yim);
       }
     }
     __syncthreads();
+    // y_i in a fixed order: the row sums of tiles (I, 0..I), then the column
+    // sums of tiles (I..T-1, I) — the same bits on every run
     float yr = 0.f, yi = 0.f;
-    if (i < n) {
-      const cf y = ys[i];
-      yr = y.x;
-      yi = y.y;
-      ys[i] = make_float2(0.f, 0.f);   // cleared for the next step (two barriers ahead)
+    if (i >= k + 1 && i < n) {
+      const int o = k + 1, T = (n - o + 31) >> 5;
+      const int I = (i - o) >> 5, l = (i - o) & 31;
+      const int t0 = I * (I + 1) / 2;
+      for (int J = 0; J <= I; ++J) {
+        const cf v = part[2 * (t0 + J) * 32 + l];
+        yr += v.x;
+        yi += v.y;
+      }
+      for (int I2 = I; I2 < T; ++I2) {
+        const cf v = part[(2 * (I2 * (I2 + 1) / 2 + I) + 1) * 32 + l];
+        yr += v.x;
+        yi += v.y;
+      }
     }
     // vᴴ y (real for Hermitian A)
     const float vy = block_sum((i >= k + 1 && i < n) ? (vi.x * yr + vi.y * yi) : 0.f,
@@ -579,12 +595,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
 
 int eig2_prepare(int nmax) {
   if (nmax > kT) return fail(MSLR_ERR_UNSUPPORTED, "Gram side above 1024");
-  const size_t sm = smem_bytes(nmax);
+  const size_t sm = smem_bytes(nmax, kT);
   if (sm > 227 * 1024) return fail(MSLR_ERR_UNSUPPORTED, "Gram side too large for the eigen stage");
   MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   if (nmax <= kSmallT)
     MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm));
+                                       (int)smem_bytes(nmax, kSmallT)));
   return MSLR_OK;
 }
 
@@ -611,9 +627,9 @@ int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int th
     nmax = std::max(nmax, segs[s].n);
   }
   if (nmax <= kSmallT)
-    k_eig<kSmallT, 2><<<(unsigned)total, kSmallT, smem_bytes(nmax), st>>>(a);
+    k_eig<kSmallT, 2><<<(unsigned)total, kSmallT, smem_bytes(nmax, kSmallT), st>>>(a);
   else
-    k_eig<kT, 1><<<(unsigned)total, kT, smem_bytes(nmax), st>>>(a);
+    k_eig<kT, 1><<<(unsigned)total, kT, smem_bytes(nmax, kT), st>>>(a);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
 }

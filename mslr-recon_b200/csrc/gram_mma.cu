@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 }  // namespace
 
 // Dynamic shared memory above 48 KB is opted into once per device.
-static int tc_prepare() {
+int tc_prepare() {
   static std::mutex mu;
   static bool done[64] = {};
   int dev = 0;

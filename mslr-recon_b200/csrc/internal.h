@@ -72,6 +72,19 @@ struct Ctx {
   bool spec = false;      // shape-specialised kernels (sense_spec.cu) exist for N
   int spec_xy_ctas = 0;   // resident CTAs of the specialised plane kernel
   int spec_zfwd_ctas = 0; // resident CTAs of the specialised forward z kernel
+  // graph-captured POGM step (tuned form): captured on a private stream the
+  // first time pogm_step sees a given X, replayed afterwards
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t gev_in = nullptr, gev_out = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  const void* gX = nullptr;
+  uint64_t glaunches = 0;
+  bool use_graph = true;
+  // launch profiling of the specialised normal operator (mslr_normal_op_profile):
+  // when on, an event is recorded before and after every kernel of every chunk
+  bool prof_on = false;
+  std::vector<cudaEvent_t> prof_ev;
+  int prof_n = 0;   // events recorded in the current profiled call
 
   // POGM
   cf* d_U = nullptr;   // (Ns, Nt, nvox)

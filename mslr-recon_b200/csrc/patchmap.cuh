@@ -56,6 +56,8 @@ __device__ __forceinline__ cf m_elem(const PatchMap& m, const cf* __restrict__ i
 // gram_mma.cu: split-precision BF16 tensor-core Gram and rebuild (tuned form).
 // mma_supported: the 32-bit offset tables of those kernels cover this map.
 bool mma_supported(const PatchMap& m);
+// Opt the tensor-core kernels into their shared memory on the current device.
+int tc_prepare();
 int gram_mma_launch(const cf* img, const PatchMap& m, int64_t np, cf* out_or_part, int nsplit,
                     int lchunk, cudaStream_t st);
 int rebuild_mma_launch(const cf* img, const cf* W, const PatchMap& m, int64_t np, cf* out,

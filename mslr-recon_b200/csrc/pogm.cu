@@ -20,6 +20,8 @@
 // that a whole iteration can be replayed from a CUDA graph.
 #include <cmath>
 
+#include <string>
+
 #include "internal.h"
 
 namespace mslr {
@@ -237,7 +239,7 @@ int pogm_begin(Ctx* c, cf* X, int niter, double L, double cutoff, double bsig, c
   return MSLR_OK;
 }
 
-int pogm_step(Ctx* c, cf* X, cudaStream_t st) {
+static int pogm_step_body(Ctx* c, cf* X, cudaStream_t st) {
   int rc;
   const int64_t E = (int64_t)c->Nt * c->nvox;
   // 1. g = A'(A Σ_k x_k − y)   (scripts/reconstruct.jl:180-183)
@@ -257,6 +259,55 @@ int pogm_step(Ctx* c, cf* X, cudaStream_t st) {
     if ((rc = patch_svst(c, k, c->d_thr, c->lambdas[k], c->d_Z + k * E, X + k * E, st)))
       return rc;
   }
+  return MSLR_OK;
+}
+
+// One POGM iteration.  In the tuned form the whole iteration (about 1400
+// kernels at 90×90×60) is captured once into a CUDA graph on the context's
+// private stream and replayed; the caller's stream is joined with events on
+// both sides, so any stream (the legacy default included) may be passed.  All
+// per-iteration scalars live in device memory (PogmState), so one graph
+// serves every iteration of every run on the same X.
+int pogm_step(Ctx* c, cf* X, cudaStream_t st) {
+  if (c->form != MSLR_FORM_TUNED || !c->use_graph) return pogm_step_body(c, X, st);
+  if (!c->gstream) {
+    MSLR_CUDA_TRY(cudaStreamCreateWithFlags(&c->gstream, cudaStreamNonBlocking));
+    MSLR_CUDA_TRY(cudaEventCreateWithFlags(&c->gev_in, cudaEventDisableTiming));
+    MSLR_CUDA_TRY(cudaEventCreateWithFlags(&c->gev_out, cudaEventDisableTiming));
+  }
+  if (!c->gexec || c->gX != X) {
+    if (c->gexec) {
+      cudaGraphExecDestroy(c->gexec);
+      c->gexec = nullptr;
+    }
+    const uint64_t l0 = c->launches;
+    MSLR_CUDA_TRY(cudaStreamBeginCapture(c->gstream, cudaStreamCaptureModeThreadLocal));
+    const int rc = pogm_step_body(c, X, c->gstream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->gstream, &g);
+    if (rc || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      c->launches = l0;
+      return rc ? rc : fail(MSLR_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&c->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      c->gexec = nullptr;
+      c->launches = l0;
+      return fail(MSLR_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    }
+    c->glaunches = c->launches - l0;
+    c->launches = l0;
+    c->gX = X;
+  }
+  MSLR_CUDA_TRY(cudaEventRecord(c->gev_in, st));
+  MSLR_CUDA_TRY(cudaStreamWaitEvent(c->gstream, c->gev_in, 0));
+  MSLR_CUDA_TRY(cudaGraphLaunch(c->gexec, c->gstream));
+  MSLR_CUDA_TRY(cudaEventRecord(c->gev_out, c->gstream));
+  MSLR_CUDA_TRY(cudaStreamWaitEvent(st, c->gev_out, 0));
+  c->launches += c->glaunches;
   return MSLR_OK;
 }
 

@@ -432,6 +432,18 @@ bool sense_spec_setup(Ctx* c) {
   return true;
 }
 
+// Records a profiling event on st when the context is profiling.
+static int prof_mark(Ctx* c, cudaStream_t st) {
+  if (!c->prof_on) return MSLR_OK;
+  if (c->prof_n == (int)c->prof_ev.size()) {
+    cudaEvent_t e;
+    MSLR_CUDA_TRY(cudaEventCreate(&e));
+    c->prof_ev.push_back(e);
+  }
+  MSLR_CUDA_TRY(cudaEventRecord(c->prof_ev[c->prof_n++], st));
+  return MSLR_OK;
+}
+
 int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
                    cudaStream_t st) {
   const SpecOps* o = find_ops(c->N[0], c->N[1], c->N[2]);
@@ -452,6 +464,7 @@ int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
     int mode = cc0 > 0 ? 1 : 0;
     for (int t0 = 0; t0 < c->Nt; t0 += F) {
       int f = std::min(F, c->Nt - t0);
+      if (int rc = prof_mark(c, st)) return rc;
       {
         const int U = Ny * f * ch;
         const int grid = std::max(1, std::min(U, c->spec_zfwd_ctas));
@@ -461,6 +474,7 @@ int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
         MSLR_CUDA_TRY(cudaLaunchKernel(o->zfwd, dim3(grid), dim3(o->zfwd_threads), args,
                                        o->smem_zfwd, st));
       }
+      if (int rc = prof_mark(c, st)) return rc;
       {
         const int units = Nz * ch * f;
         const int grid = std::max(1, std::min(units, c->spec_xy_ctas));
@@ -469,6 +483,7 @@ int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
         MSLR_CUDA_TRY(
             cudaLaunchKernel(o->xy, dim3(grid), dim3(o->xy_threads), args, o->smem_xy, st));
       }
+      if (int rc = prof_mark(c, st)) return rc;
       {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(ch, Ny, f);
@@ -488,6 +503,7 @@ int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
                         (void*)&sub,  (void*)&c->d_tw[2], (void*)&err};
         MSLR_CUDA_TRY(cudaLaunchKernelExC(&cfg, o->zadj, args));
       }
+      if (int rc = prof_mark(c, st)) return rc;
       c->launches += 3;
     }
   }

@@ -498,6 +498,7 @@ int svst_setup(Ctx* c) {
   if ((rc = dalloc(c, (void**)&c->d_img_tmp, (size_t)c->Nt * c->nvox * sizeof(cf)))) return rc;
   int nmax = 1;
   for (auto& g : c->scales) nmax = std::max(nmax, g.n);
+  if ((rc = tc_prepare())) return rc;   // before any graph capture of the iteration
   return eig2_prepare(nmax);
 }
 

@@ -40,6 +40,21 @@ def normal_op_flops(nvox: int, Nt: int, Nc: int) -> float:
     return 2.0 * Nc * Nt * 5.0 * nvox * math.log2(nvox)
 
 
+def plane_pass_bytes(Nx: int, Ny: int, planes: int) -> int:
+    """Plane kernel (x/y transforms, mask, inverse): every k-space plane of
+    the chunk is read once and written once, plus its sampling bits."""
+    pl = Nx * Ny
+    return planes * (2 * pl * C64 + (pl + 31) // 32 * 4)
+
+
+def plane_pass_flops(Nx: int, Ny: int, planes: int) -> float:
+    """Nominal 5 N log2 N for the forward and the backward 2-D transform of
+    each plane (N = Nx·Ny)."""
+    import math
+    pl = Nx * Ny
+    return planes * 2 * 5.0 * pl * math.log2(pl)
+
+
 def svst_bytes(nvox: int, Nt: int) -> int:
     """One scale's patch SVST: read the scale image, write it back."""
     return 2 * nvox * Nt * C64

@@ -203,6 +203,30 @@ def test_small_workload_per_iteration_parity(torch, M, small_problem):
             assert ctx.pogm_restarts() == restarts, form
 
 
+def test_graph_replay_is_bit_identical(torch, M, small_problem):
+    """Tuned form: the graph-captured iteration (default) and direct kernel
+    launches give bit-identical iterates and restart flags, and the graph is
+    re-captured when the iterate moves to another buffer."""
+    pb = small_problem
+    Nt, Nc, K = pb["y"].shape
+    outs = []
+    for graph in (True, False):
+        with M.MSLRContext(pb["N"], Nc, Nt, K, pb["patch_sizes"], pb["strides"], form="tuned") as ctx:
+            ctx.set_graph(graph)
+            ctx.bind(dev(torch, pb["smaps"]), dev(torch, pb["y"]), dev(torch, pb["idx"], torch.int32))
+            X = ctx.init_x0()
+            ctx.pogm_begin(X, 6, L=1.0)
+            for _ in range(3):
+                ctx.pogm_step(X)
+            X2 = X.clone()              # continue on another buffer
+            for _ in range(3):
+                ctx.pogm_step(X2)
+            torch.cuda.synchronize()
+            outs.append((X2.cpu().numpy(), ctx.pogm_restarts()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1] == outs[1][1]
+
+
 # --- errors -------------------------------------------------------------------------
 def test_bad_indices_rejected(torch, M, gold):
     Nt, Nc, K = gold["y"].shape
