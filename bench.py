@@ -40,6 +40,18 @@ PLANE_TRAFFIC_PER_LAUNCH = 47254016 + 2285056
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
+def describe(pb) -> str:
+    """Workload label, e.g. "90x90x60, 18 coils, Nt=300, scales [90,90,60]+[10,10,10] stride=size"."""
+    Nt, Nc, _ = pb["y"].shape
+    sc = "+".join("[%s]" % ",".join(str(v) for v in ps) for ps in pb["patch_sizes"])
+    st = ("stride=size" if all(list(a) == list(b) for a, b in zip(pb["patch_sizes"], pb["strides"]))
+          else "strides " + "+".join("[%s]" % ",".join(str(v) for v in ss) for ss in pb["strides"]))
+    return f"{'x'.join(str(v) for v in pb['N'])}, {Nc} coils, Nt={Nt}, scales {sc} {st}"
+
+
+METRIC = "POGM iter/s (90x90x60, 18 coils, Nt=300, 2 scales)"
+
+
 def load_problem(name: str, seed_offset: int = 0):
     """Seeded synthetic problem of the named workload (the generator module is
     loaded by path so that the CPU-only reference arm needs no GPU library)."""
@@ -212,11 +224,11 @@ def run_reference(args):
         if i >= args.warmup:
             secs.append(s)
     v = 1.0 / (sum(secs) / len(secs))
-    line = {"metric": "POGM iter/s (90x90x60, 18 coils, Nt=300, 2 scales)", "value": v,
+    line = {"metric": METRIC, "value": v,
             "unit": "iter/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-            "config": {"workload": "90x90x60, 18 coils, Nt=300, scales [90,90,60]+[10,10,10] stride=size"},
+            "config": {"workload": describe(pb)},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "iter/s", "cores": cores, "kind": "port", "sample": desc},
             "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -398,13 +410,13 @@ def main():
     if world > 1:
         dist.barrier()
     if rank == 0:
-        line = {"metric": "POGM iter/s (90x90x60, 18 coils, Nt=300, 2 scales)", "value": value,
+        line = {"metric": METRIC, "value": value,
                 "unit": "iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-                "config": {"workload": "90x90x60, 18 coils, Nt=300, scales [90,90,60]+[10,10,10] stride=size",
+                "config": {"workload": describe(pb),
                            "form": args.form, "parallelism": f"replicas x{world}",
-                           "l2": "inputs larger than L2 (X is 2.3 GB)",
+                           "l2": f"inputs larger than L2 (X is {pb['y'].shape[0] * nvox * 8 * len(pb['patch_sizes']) / 1e9:.1f} GB)",
                            "plain_form_iter_s": plain_ips,
                            "tuned_over_plain": (value / world / plain_ips * world) if plain_ips else None,
                            "phases": phases},

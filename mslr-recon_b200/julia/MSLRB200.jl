@@ -1,0 +1,189 @@
+"""
+    MSLRB200
+
+Julia binding of `libmslr.so` (the C ABI in `include/mslr.h`): drop-in
+replacements for the per-iteration path of `run_recon`
+(`scripts/reconstruct.jl`) — the SENSE operator `Asense_gpu`
+(`src/sense_gpu.jl:56-108`), `dc_cost_grad` (`scripts/reconstruct.jl:180-183`),
+`patchSVST_gpu` (`src/sense_gpu.jl:138-160`), `pogm_mod` with `mom=:pogm,
+restart=:gr` (`src/mirt_mod.jl:74-188`) and `poweriter_mod`
+(`src/mirt_mod.jl:215-238`).
+
+Arrays are `CuArray{ComplexF32}` in the reference's column-major layouts:
+image `(Nx,Ny,Nz,Nt)`, `X` `(Nx,Ny,Nz,Nt,Ns)`, coil maps `(Nx,Ny,Nz,Nc)`,
+k-space `(K,Nc,Nt)`, sample indices `(K,Nt)` 1-based `Int32`.  Every call
+runs on CUDA.jl's task-local stream.  Library errors are raised as
+`ArgumentError` (bad arguments, as the reference does) or `MSLRError`.
+"""
+module MSLRB200
+
+using CUDA
+
+export MSLRContext, sense_forward!, sense_adjoint!, dc_cost_grad!, patch_svst!,
+       pogm_run!, power_iter, mslr_lambdas
+
+const libmslr = get(ENV, "MSLR_LIB", joinpath(@__DIR__, "..", "libmslr.so"))
+
+struct MSLRError <: Exception
+    code::Int32
+    msg::String
+end
+
+const FORM_PLAIN = Int32(0)
+const FORM_TUNED = Int32(1)
+
+_stream() = CUDA.stream().handle   # cudaStream_t of the task-local stream
+
+function _check(rc::Integer, h::Ptr{Cvoid}=C_NULL)
+    rc == 0 && return nothing
+    msg = unsafe_string(ccall((:mslr_last_error, libmslr), Cstring, (Ptr{Cvoid},), h))
+    rc == 1 && throw(ArgumentError(msg))
+    throw(MSLRError(Int32(rc), msg))
+end
+
+"""
+    MSLRContext(N, Nc, Nt, K, patch_sizes, strides; form=:tuned)
+
+The state `run_recon` builds (scripts/reconstruct.jl:133-214) for
+`length(patch_sizes)` scales.  Free with `close(ctx)` (or let the GC do it).
+"""
+mutable struct MSLRContext
+    h::Ptr{Cvoid}
+    N::NTuple{3,Int}
+    Nc::Int
+    Nt::Int
+    K::Int
+    Ns::Int
+    niter::Int
+end
+
+function MSLRContext(N, Nc::Integer, Nt::Integer, K::Integer, patch_sizes, strides;
+                     form::Symbol=:tuned)
+    length(patch_sizes) == length(strides) ||
+        throw(ArgumentError("patch_sizes and strides differ in length"))
+    ps = Int32[p for s in patch_sizes for p in s]
+    ss = Int32[p for s in strides for p in s]
+    out = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:mslr_create, libmslr), Cint,
+               (Ptr{Int32}, Int32, Int32, Int64, Int32, Ptr{Int32}, Ptr{Int32}, Int32,
+                Ptr{Ptr{Cvoid}}),
+               Int32[N...], Nc, Nt, K, length(patch_sizes), ps, ss,
+               form === :tuned ? FORM_TUNED : FORM_PLAIN, out)
+    _check(rc)
+    ctx = MSLRContext(out[], Tuple(Int.(N)), Int(Nc), Int(Nt), Int(K), length(patch_sizes), 0)
+    finalizer(close, ctx)
+    return ctx
+end
+
+function Base.close(ctx::MSLRContext)
+    if ctx.h != C_NULL
+        ccall((:mslr_destroy, libmslr), Cint, (Ptr{Cvoid},), ctx.h)
+        ctx.h = C_NULL
+    end
+    return nothing
+end
+
+"""
+    bind!(ctx, smaps, ksp, idx)
+
+Bind the acquisition: SOS-normalised coil maps `(Nx,Ny,Nz,Nc)`, k-space
+`(K,Nc,Nt)` and 1-based sample indices `(K,Nt)` (`findall(vec(Ω_t))` per
+frame, scripts/reconstruct.jl:144-147).  The library keeps its own copies.
+"""
+function bind!(ctx::MSLRContext, smaps::CuArray{ComplexF32}, ksp::CuArray{ComplexF32},
+               idx::CuArray{Int32})
+    size(smaps) == (ctx.N..., ctx.Nc) || throw(ArgumentError("smaps size $(size(smaps))"))
+    size(ksp) == (ctx.K, ctx.Nc, ctx.Nt) || throw(ArgumentError("ksp size $(size(ksp))"))
+    size(idx) == (ctx.K, ctx.Nt) || throw(ArgumentError("idx size $(size(idx))"))
+    _check(ccall((:mslr_bind, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, CuPtr{ComplexF32}, CuPtr{Int32}, Int32, Ptr{Cvoid}),
+                 ctx.h, smaps, ksp, idx, Int32(1), _stream()), ctx.h)
+    return ctx
+end
+
+"""A * x over all frames (Asense_gpu fwd per frame, block_diag)."""
+function sense_forward!(y::CuArray{ComplexF32}, ctx::MSLRContext, x::CuArray{ComplexF32})
+    _check(ccall((:mslr_sense_forward, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, CuPtr{ComplexF32}, Ptr{Cvoid}),
+                 ctx.h, x, y, _stream()), ctx.h)
+    return y
+end
+
+"""A' * y (exact unitary adjoint, src/sense_gpu.jl:84-101)."""
+function sense_adjoint!(x::CuArray{ComplexF32}, ctx::MSLRContext, y::CuArray{ComplexF32})
+    _check(ccall((:mslr_sense_adjoint, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, CuPtr{ComplexF32}, Ptr{Cvoid}),
+                 ctx.h, y, x, _stream()), ctx.h)
+    return x
+end
+
+"""
+    dc_cost_grad!(g, ctx, X)
+
+`A'(A Σ_k X[..,k] − y)` into `g` `(Nx,Ny,Nz,Nt)`; the reference then
+`repeat`s it over the scales (scripts/reconstruct.jl:180-183).
+"""
+function dc_cost_grad!(g::CuArray{ComplexF32}, ctx::MSLRContext, X::CuArray{ComplexF32})
+    _check(ccall((:mslr_normal_op, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, Int32, CuPtr{ComplexF32}, Int32, Ptr{Cvoid}),
+                 ctx.h, X, Int32(size(X, 5)), g, Int32(1), _stream()), ctx.h)
+    return g
+end
+
+"""
+    patch_svst!(out, ctx, img, k, β)
+
+`patchSVST_gpu(img, β, PATCH_SIZES[k], STRIDES[k])` for scale `k` (1-based)
+into `out` (may be `img`: the reference's g_prox writes in place).
+"""
+function patch_svst!(out::CuArray{ComplexF32}, ctx::MSLRContext, img::CuArray{ComplexF32},
+                     k::Integer, β::Real)
+    _check(ccall((:mslr_patch_svst, libmslr), Cint,
+                 (Ptr{Cvoid}, Int32, Float64, CuPtr{ComplexF32}, CuPtr{ComplexF32}, Ptr{Cvoid}),
+                 ctx.h, Int32(k - 1), Float64(β), img, out, _stream()), ctx.h)
+    return out
+end
+
+"""
+    pogm_run!(ctx, X, niter, L; restart_cutoff=0.0, bsig=1.0) -> restarts
+
+`pogm_mod(X, ..., dc_cost_grad, L; mom=:pogm, restart=:gr, niter, g_prox)`
+with run_recon's closures, overwriting `X` `(Nx,Ny,Nz,Nt,Ns)`.  Returns the
+per-iteration restart flags (entry 1 is false, as the logger's first entry).
+Cost logging is not computed.
+"""
+function pogm_run!(ctx::MSLRContext, X::CuArray{ComplexF32}, niter::Integer, L::Real;
+                   restart_cutoff::Real=0.0, bsig::Real=1.0)
+    flags = zeros(UInt8, niter + 1)
+    _check(ccall((:mslr_pogm_run, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, Int32, Float64, Float64, Float64, Ptr{UInt8},
+                  Ptr{Cvoid}),
+                 ctx.h, X, Int32(niter), Float64(L), Float64(restart_cutoff), Float64(bsig),
+                 flags, _stream()), ctx.h)
+    return Bool.(flags)
+end
+
+"""X0 of scripts/reconstruct.jl:209-214: X[..,1] = A'y, other scales 0."""
+function init_x0!(ctx::MSLRContext, X::CuArray{ComplexF32})
+    _check(ccall((:mslr_init_x0, libmslr), Cint, (Ptr{Cvoid}, CuPtr{ComplexF32}, Ptr{Cvoid}),
+                 ctx.h, X, _stream()), ctx.h)
+    return X
+end
+
+"""σ₁(A) by poweriter_mod (src/mirt_mod.jl:215-238), x0 = ones."""
+function power_iter(ctx::MSLRContext; niter::Integer=200, tol::Real=1e-6)
+    s1 = Ref{Float64}(0.0)
+    it = Ref{Int32}(0)
+    _check(ccall((:mslr_power_iter, libmslr), Cint,
+                 (Ptr{Cvoid}, Int32, Float64, Ref{Float64}, Ref{Int32}, Ptr{Cvoid}),
+                 ctx.h, Int32(niter), Float64(tol), s1, it, _stream()), ctx.h)
+    return s1[], Int(it[])
+end
+
+"""Ong–Lustig λ_k of scripts/reconstruct.jl:164-169."""
+function mslr_lambdas(N, Nt::Integer, patch_sizes)
+    return [sqrt(prod(ps)) + sqrt(Nt) + sqrt(log(prod(N) * Nt / max(prod(ps), Nt)))
+            for ps in patch_sizes]
+end
+
+end # module
