@@ -167,6 +167,16 @@ int mslr_normal_op_profile(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g,
 int mslr_patch_svst(mslr_ctx* ctx, int32_t scale, double beta, const void* img_in,
                     void* img_out, void* stream);
 
+/* The two terms of run_recon's cost (scripts/reconstruct.jl:176-194,
+ * logged each iteration by its logger, :205) for X (Nx,Ny,Nz,Nt,ns_in):
+ *   dc_cost  = ½ ‖A Σ_k X[..,k] − y‖²
+ *   reg_cost = Σ_k λ_k · patch_nucnorm(img2patches(X[..,k]))  (ns_in == n_scales)
+ * FP64 sums.  dc_cost is formed from one normal operator, A'y and ‖y‖²
+ * (kept from bind); reg_cost from the eigenvalues of every patch's Gram
+ * matrix.  Either output pointer may be NULL.  Synchronises `stream`. */
+int mslr_cost(mslr_ctx* ctx, const void* X, int32_t ns_in, double* dc_cost, double* reg_cost,
+              void* stream);
+
 /* X0 of scripts/reconstruct.jl:209-214: X[..,1] = A'y, other scales 0. */
 int mslr_init_x0(mslr_ctx* ctx, void* X, void* stream);
 

@@ -46,6 +46,7 @@ SIGNATURES = {
     "mslr_sense_adjoint": (C.c_int, [_P, _P, _P, _P]),
     "mslr_normal_op": (C.c_int, [_P, _P, _I32, _P, _I32, _P]),
     "mslr_set_graph": (C.c_int, [_P, _I32]),
+    "mslr_cost": (C.c_int, [_P, _P, _I32, C.POINTER(C.c_double), C.POINTER(C.c_double), _P]),
     "mslr_normal_op_profile": (C.c_int, [_P, _P, _I32, _P, _P, C.POINTER(C.c_double),
                                          C.POINTER(C.c_int64)]),
     "mslr_patch_svst": (C.c_int, [_P, _I32, _D, _P, _P, _P]),

@@ -148,6 +148,20 @@ class MSLRContext:
                                      1 if subtract_data else 0, _stream_ptr(stream)))
         return g
 
+    def cost(self, X: torch.Tensor, stream=None):
+        """(dc_cost, reg_cost) of run_recon's logger (scripts/reconstruct.jl:176-194)
+        for X (Ns, Nt, Nz, Ny, Nx); FP64."""
+        import ctypes as C
+        if X.dim() == 4:
+            X = X.unsqueeze(0)
+        ns = X.shape[0]
+        _dev_c64(X, (ns,) + self.img_shape, "X")
+        dc = C.c_double()
+        reg = C.c_double()
+        self._chk(lib.mslr_cost(self._h, X.data_ptr(), ns, C.byref(dc),
+                                C.byref(reg) if ns == self.Ns else None, _stream_ptr(stream)))
+        return float(dc.value), (float(reg.value) if ns == self.Ns else None)
+
     def set_graph(self, enable: bool):
         """Tuned form: replay the POGM iteration from a captured CUDA graph
         (default) or launch its kernels directly."""

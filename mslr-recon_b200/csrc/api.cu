@@ -53,6 +53,10 @@ static void free_ctx(mslr_ctx* c) {
   if (c->gev_in) cudaEventDestroy(c->gev_in);
   if (c->gev_out) cudaEventDestroy(c->gev_out);
   if (c->gstream) cudaStreamDestroy(c->gstream);
+  if (c->d_nuc) cudaFree(c->d_nuc);
+  if (c->d_zero) cudaFree(c->d_zero);
+  if (c->d_cost_g) cudaFree(c->d_cost_g);
+  if (c->d_cost_part) cudaFree(c->d_cost_part);
   delete c;
 }
 
@@ -388,6 +392,20 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
     return ctx_fail(ctx, fail(MSLR_ERR_NONFINITE, "non-finite value in the POGM restart sums"));
   if (herr & 8)
     return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a device-side wait for a bulk copy timed out"));
+  return MSLR_OK;
+}
+
+int mslr_cost(mslr_ctx* ctx, const void* X, int32_t ns_in, double* dc_cost, double* reg_cost,
+              void* stream) {
+  CTX_CHECK(ctx);
+  NEED_BOUND(ctx);
+  if (!X || ns_in <= 0) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad argument"));
+  if (reg_cost && ns_in != ctx->Ns)
+    return ctx_fail(ctx, fail(MSLR_ERR_ARG, "reg_cost needs one image per scale (ns_in == n_scales)"));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const cf* Xc = reinterpret_cast<const cf*>(X);
+  if (dc_cost) CTX_RET(ctx, dc_cost_eval(ctx, Xc, ns_in, dc_cost, st));
+  if (reg_cost) CTX_RET(ctx, patch_nucnorm_all(ctx, Xc, reg_cost, st));
   return MSLR_OK;
 }
 

@@ -97,6 +97,7 @@ struct Seg {
   double* aux;     // np × n × n: FP64 pivots of the twisted factorisations
   int* rank;       // np
   double lam;      // threshold multiplier of the segment (λ_k)
+  double* nuc;     // values-only mode when set: np sums Σ √λ_i over λ_i above β², no vectors
 };
 
 constexpr int kMaxSeg = 8;
@@ -399,6 +400,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     hv[tid] = (sg > beta_d && sg > 0.0) ? (float)((sg - beta_d) / sg) : 0.f;
   }
   __syncthreads();
+  if (S.nuc) {   // nuclear norm of the patch (src/recon.jl:138-146): Σ σ_i = Σ √λ_i
+    const double sq = (tid < r) ? sqrt(fmax(lam[tid], 0.0)) : 0.0;
+    const double tot = block_sum_d(sq, redd);
+    if (tid == 0) S.nuc[ip] = tot;
+    return;
+  }
   if (r == 0) {
     for (int64_t q = tid; q < (int64_t)n * n; q += kT) Z[q] = make_float2(0.f, 0.f);
     return;
@@ -623,6 +630,7 @@ int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int th
     S.aux = segs[s].aux;
     S.rank = segs[s].rank;
     S.lam = segs[s].lam;
+    S.nuc = segs[s].nuc;
     total += segs[s].np;
     nmax = std::max(nmax, segs[s].n);
   }
@@ -644,6 +652,7 @@ int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, cons
   s.aux = reinterpret_cast<double*>(aux);
   s.rank = rank;
   s.lam = lam;
+  s.nuc = nullptr;
   return eig_launch_multi(1, &s, thr, thr_per_patch, st);
 }
 

@@ -59,6 +59,12 @@ struct Ctx {
   int nwords = 0;
   int32_t* d_idx = nullptr;    // (Nt, K) 0-based
   cf* d_ahy = nullptr;         // (Nt, nvox) A'y
+  double ynorm2 = 0.0;         // ‖y‖² (FP64) of the bound k-space, for dc_cost
+  double* d_nuc = nullptr;     // per-patch nuclear norms (cost evaluation)
+  int64_t nuc_cap = 0;
+  double* d_zero = nullptr;    // device 0.0 (threshold of the values-only eigen mode)
+  cf* d_cost_g = nullptr;      // gradient scratch of the cost evaluation (Nt, nvox)
+  double* d_cost_part = nullptr;   // FP64 block partials of the cost inner products
   cf* d_T = nullptr;           // (F, Nc, nvox) per-coil k-space of a chunk of frames
   int F = 1;
   bool bound = false;
@@ -156,12 +162,18 @@ struct EigSegment {
   double* aux;   // np × n × n scratch
   int* rank;     // np
   double lam;
+  double* nuc = nullptr;   // when set: per-patch Σ √λ above the threshold only (no vectors, no W)
 };
 int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int thr_per_patch,
                      cudaStream_t st);
 int eig2_prepare(int nmax);
 int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, const double* thr,
                 int thr_per_patch, double lam, cudaStream_t st);
+
+// ---- cost evaluation (svst.cu, cost.cu) ------------------------------------------
+int patch_nucnorm_all(Ctx* c, const cf* X, double* reg_out, cudaStream_t st);
+int data_norm2(Ctx* c, const cf* y, double* out, cudaStream_t st);
+int dc_cost_eval(Ctx* c, const cf* X, int ns, double* dc_out, cudaStream_t st);
 
 // ---- pogm.cu -----------------------------------------------------------------
 int pogm_setup(Ctx* c);

@@ -373,6 +373,7 @@ int sense_bind(Ctx* c, const cf* smaps, const cf* y, const int32_t* idx, int bas
   MSLR_CUDA_TRY(cudaGetLastError());
   c->bound = true;
   rc = sense_adjoint(c, y, c->d_ahy, st);
+  if (!rc) rc = data_norm2(c, y, &c->ynorm2, st);   // ‖y‖² for dc_cost (cost.cu)
   if (rc) {
     c->bound = false;
     return rc;

@@ -699,4 +699,58 @@ int svst_batch_noalloc(int mrows, int ncols, int batch, const double* betas, con
                     MSLR_FORM_TUNED, st);
 }
 
+// reg_cost of run_recon (scripts/reconstruct.jl:185-194): Σ_k λ_k Σ_patches
+// Σ σ(P_p(X_k)) (patch_nucnorm, src/recon.jl:138-146).  The singular values of
+// each patch are the square roots of its Gram's eigenvalues: Grams of every
+// patch, then the eigen stage in values-only mode (tridiagonalisation and FP64
+// bisection, no vectors).  Per-patch sums come back to the host and are added
+// in patch order in FP64.  Synchronises st.
+int patch_nucnorm_all(Ctx* c, const cf* X, double* reg_out, cudaStream_t st) {
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  int64_t npmax = 0;
+  for (auto& g : c->scales) npmax = std::max(npmax, g.Np);
+  int rc;
+  if (c->nuc_cap < npmax) {
+    if (c->d_nuc) cudaFree(c->d_nuc);
+    c->d_nuc = nullptr;
+    c->nuc_cap = 0;
+    if ((rc = dalloc(c, (void**)&c->d_nuc, (size_t)npmax * sizeof(double)))) return rc;
+    c->nuc_cap = npmax;
+  }
+  if (!c->d_zero) {
+    if ((rc = dalloc(c, (void**)&c->d_zero, sizeof(double)))) return rc;
+    MSLR_CUDA_TRY(cudaMemsetAsync(c->d_zero, 0, sizeof(double), st));
+  }
+  const bool tc = (c->form == MSLR_FORM_TUNED);
+  std::vector<double> h;
+  double reg = 0.0;
+  for (int k = 0; k < c->Ns; ++k) {
+    const ScaleGeom& g = c->scales[k];
+    const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
+    const int nsplit = choose_split(g.Np, g.n, g.L);
+    WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? k : 0].gram, g.Np, g.n, nsplit);
+    if ((rc = svst_gram(X + k * E, m, g.Np, w, nsplit, tc, st, &c->launches))) return rc;
+    EigSegment seg;
+    seg.n = g.n;
+    seg.np = g.Np;
+    seg.gram = w.gram;
+    seg.zv = reinterpret_cast<cf*>(w.zv);
+    seg.aux = w.aux;
+    seg.rank = w.rank;
+    seg.lam = 0.0;
+    seg.nuc = c->d_nuc;
+    if ((rc = eig_launch_multi(1, &seg, c->d_zero, 0, st))) return rc;
+    c->launches += 1;
+    h.resize((size_t)g.Np);
+    MSLR_CUDA_TRY(cudaMemcpyAsync(h.data(), c->d_nuc, (size_t)g.Np * sizeof(double),
+                                  cudaMemcpyDeviceToHost, st));
+    MSLR_CUDA_TRY(cudaStreamSynchronize(st));
+    double sk = 0.0;
+    for (double v : h) sk += v;
+    reg += c->lambdas[k] * sk;
+  }
+  *reg_out = reg;
+  return MSLR_OK;
+}
+
 }  // namespace mslr

@@ -21,13 +21,16 @@ def sos_normalize(smaps: np.ndarray) -> np.ndarray:
 
 def run_recon(smaps, y, idx, patch_sizes, strides, niters: int, sigma1=None, form: str = "tuned",
               index_base: int = 0, power_niter: int = 200, power_tol: float = 1e-6,
-              restart_cutoff: float = 0.0, bsig: float = 1.0, return_components: bool = True):
+              restart_cutoff: float = 0.0, bsig: float = 1.0, return_components: bool = True,
+              log_costs: bool = False):
     """Arguments are host numpy arrays or CUDA tensors in the layouts of
     :mod:`context`.  ``sigma1=None`` runs the power iteration (as
     σ1A_PRECOMPUTED = nothing, scripts/reconstruct.jl:152-158).
 
     Returns a dict with X (Ns,Nt,Nz,Ny,Nx), X_recon, restarts, lambdas,
-    sigma1A and L, all on the host.
+    sigma1A and L, all on the host.  With ``log_costs`` it also returns
+    dc_costs and reg_costs: the logger's (dc_cost, reg_cost) at X0 and after
+    every iteration (scripts/reconstruct.jl:204-205, :227-230).
     """
     dev = torch.device("cuda")
     smaps_t = torch.as_tensor(smaps).to(dev, torch.complex64).contiguous()
@@ -41,7 +44,18 @@ def run_recon(smaps, y, idx, patch_sizes, strides, niters: int, sigma1=None, for
             sigma1, _ = ctx.power_iter(power_niter, power_tol)
         L = ctx.Ns * float(sigma1) ** 2
         X = ctx.init_x0()
-        restarts = ctx.pogm_run(X, niters, L, restart_cutoff, bsig)
+        dcs, regs = [], []
+        if log_costs:
+            ctx.pogm_begin(X, niters, L, restart_cutoff, bsig)
+            for it in range(niters + 1):
+                if it:
+                    ctx.pogm_step(X)
+                dc, reg = ctx.cost(X)
+                dcs.append(dc)
+                regs.append(reg)
+            restarts = ctx.pogm_restarts()
+        else:
+            restarts = ctx.pogm_run(X, niters, L, restart_cutoff, bsig)
         torch.cuda.synchronize()
         out = {
             "X_recon": X.sum(dim=0).cpu().numpy(),
@@ -54,6 +68,9 @@ def run_recon(smaps, y, idx, patch_sizes, strides, niters: int, sigma1=None, for
             "strides": ctx.strides,
             "Niters": niters,
         }
+        if log_costs:
+            out["dc_costs"] = dcs
+            out["reg_costs"] = regs
         if return_components:
             out["X"] = X.cpu().numpy()
     return out

@@ -203,6 +203,26 @@ def test_small_workload_per_iteration_parity(torch, M, small_problem):
             assert ctx.pogm_restarts() == restarts, form
 
 
+@pytest.mark.parametrize("form", ["plain", "tuned"])
+def test_costs_per_iteration_vs_oracle(torch, M, small_problem, form):
+    """run_recon's logged costs (dc_cost, reg_cost at X0 and after every
+    iteration, scripts/reconstruct.jl:176-205) against the FP64 oracle on the
+    small workload, within 1e-4 relative."""
+    pb = small_problem
+    niter = 6
+    prob = O.ReconProblem(smaps=pb["smaps"].astype(np.complex128), idx=pb["idx"],
+                          y=pb["y"].astype(np.complex128), patch_sizes=pb["patch_sizes"],
+                          strides=pb["strides"], sigma1=1.0)
+    _, _, dcs, regs = O.run_recon_arrays(prob, niter, log_costs=True)
+    out = M.run_recon(pb["smaps"], pb["y"], pb["idx"], pb["patch_sizes"], pb["strides"], niter,
+                      sigma1=1.0, form=form, log_costs=True, return_components=False)
+    assert len(out["dc_costs"]) == niter + 1 == len(dcs)
+    for a, b in zip(out["dc_costs"], dcs):
+        assert a == pytest.approx(b, rel=1e-4), (form, out["dc_costs"], dcs)
+    for a, b in zip(out["reg_costs"], regs):
+        assert a == pytest.approx(b, rel=1e-4), (form, out["reg_costs"], regs)
+
+
 def test_graph_replay_is_bit_identical(torch, M, small_problem):
     """Tuned form: the graph-captured iteration (default) and direct kernel
     launches give bit-identical iterates and restart flags, and the graph is
