@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "internal.h"
+#include "patchmap.cuh"
 
 struct mslr_ctx : public mslr::Ctx {};
 
@@ -392,6 +393,10 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
     return ctx_fail(ctx, fail(MSLR_ERR_NONFINITE, "non-finite value in the POGM restart sums"));
   if (herr & 8)
     return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a device-side wait for a bulk copy timed out"));
+  int uerr = 0;
+  CTX_RET(ctx, umma_take_error(&uerr));
+  if (uerr)
+    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a tensor-core kernel's wait for its MMAs timed out"));
   return MSLR_OK;
 }
 

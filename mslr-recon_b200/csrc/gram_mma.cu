@@ -69,8 +69,9 @@ __device__ __forceinline__ uint32_t mul_plus_i(uint32_t v) {
   return ((v >> 16) | (v << 16)) ^ 0x00008000u;
 }
 
+// Not volatile: the scheduler may interleave independent products.
 __device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b) {
-  asm volatile(
+  asm(
       "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
       "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
       : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
@@ -176,15 +177,20 @@ __device__ __forceinline__ void mma_chunk(const Smem& s, const uint32_t* bh, con
       ldsm_x4(fal, s.al + o);
       ldsm_x4(frh, s.rh + o);
       ldsm_x4(frl, s.rl + o);
+      // the three split products of an accumulator are 8 MMAs apart, so no
+      // MMA waits on the one before it
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        mma_bf16(cr[i][j], fah, fbh[j]);
-        mma_bf16(cr[i][j], fah, fbl[j]);
-        mma_bf16(cr[i][j], fal, fbh[j]);
-        mma_bf16(ci[i][j], frh, fbh[j]);
-        mma_bf16(ci[i][j], frh, fbl[j]);
-        mma_bf16(ci[i][j], frl, fbh[j]);
-      }
+      for (int j = 0; j < 4; ++j) mma_bf16(cr[i][j], fah, fbh[j]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mma_bf16(ci[i][j], frh, fbh[j]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mma_bf16(cr[i][j], fah, fbl[j]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mma_bf16(ci[i][j], frh, fbl[j]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mma_bf16(cr[i][j], fal, fbh[j]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) mma_bf16(ci[i][j], frl, fbh[j]);
     }
   }
 }

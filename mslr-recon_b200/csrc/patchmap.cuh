@@ -58,6 +58,17 @@ __device__ __forceinline__ cf m_elem(const PatchMap& m, const cf* __restrict__ i
 bool mma_supported(const PatchMap& m);
 // Opt the tensor-core kernels into their shared memory on the current device.
 int tc_prepare();
+
+// gram_umma.cu: the same products on tcgen05 (tuned form, default)
+int gram_umma_launch(const cf* img, const PatchMap& m, int64_t np, cf* out_or_part, int nsplit,
+                     int lchunk, cudaStream_t st);
+int rebuild_umma_launch(const cf* img, const cf* W, const PatchMap& m, int64_t np, cf* out,
+                        int direct, cudaStream_t st);
+int umma_prepare();
+// Reads and clears the tcgen05 kernels' error bits (16: a bounded wait timed out).
+int umma_take_error(int* flags);
+// Tensor-core path of the tuned form: tcgen05 unless MSLR_TENSOR_PATH=mma.
+bool use_umma();
 int gram_mma_launch(const cf* img, const PatchMap& m, int64_t np, cf* out_or_part, int nsplit,
                     int lchunk, cudaStream_t st);
 int rebuild_mma_launch(const cf* img, const cf* W, const PatchMap& m, int64_t np, cf* out,

@@ -23,10 +23,22 @@
 #include <cmath>
 #include <mutex>
 
+#include <cstdlib>
+#include <string>
+
 #include "internal.h"
 #include "patchmap.cuh"
 
 namespace mslr {
+
+bool use_umma() {
+  static const bool v = [] {
+    const char* e = std::getenv("MSLR_TENSOR_PATH");
+    return !(e && std::string(e) == "mma");
+  }();
+  return v;
+}
+
 
 namespace {
 
@@ -311,7 +323,8 @@ int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
   const int lchunk = (nsplit > 1) ? ((m.L + nsplit - 1) / nsplit + 31) / 32 * 32 : m.L;
   cf* dst = (nsplit > 1) ? w.part : w.gram;
   if (tc && mma_supported(m)) {
-    int rc = gram_mma_launch(in, m, np, dst, nsplit, lchunk, st);
+    int rc = use_umma() ? gram_umma_launch(in, m, np, dst, nsplit, lchunk, st)
+                        : gram_mma_launch(in, m, np, dst, nsplit, lchunk, st);
     if (rc) return rc;
   } else {
     k_gram<<<dim3(ntri, (unsigned)np, nsplit), 256, 0, st>>>(in, m, dst, nsplit, lchunk);
@@ -325,7 +338,9 @@ int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
 int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, cf* out,
                  int direct, bool tc, cudaStream_t st, uint64_t* launches) {
   if (launches) *launches += 1;
-  if (tc && mma_supported(m)) return rebuild_mma_launch(in, w.gram, m, np, out, direct, st);
+  if (tc && mma_supported(m))
+    return use_umma() ? rebuild_umma_launch(in, w.gram, m, np, out, direct, st)
+                      : rebuild_mma_launch(in, w.gram, m, np, out, direct, st);
   const int n = m.n;
   k_rebuild<<<dim3((n + kTile - 1) / kTile, (m.L + kTile - 1) / kTile, (unsigned)np), 256, 0, st>>>(
       in, w.gram, m, out, direct);
@@ -499,6 +514,7 @@ int svst_setup(Ctx* c) {
   int nmax = 1;
   for (auto& g : c->scales) nmax = std::max(nmax, g.n);
   if ((rc = tc_prepare())) return rc;   // before any graph capture of the iteration
+  if ((rc = umma_prepare())) return rc;
   return eig2_prepare(nmax);
 }
 
