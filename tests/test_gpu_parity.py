@@ -107,6 +107,27 @@ def test_svst_batch_vs_oracle(torch, M, m, n, batch, form):
             assert rel(out[b], ref) < SVST_TOL[form], (b, rel(out[b], ref))
 
 
+@pytest.mark.parametrize("form", ["plain", "tuned"])
+def test_svst_batch_full_scale(torch, M, form):
+    """The 10³ scale of the workload as one batch: 486 patches of 1000 × 300
+    (Gram side 300), rank-8 signal + noise, thresholds inside the spectrum;
+    three patches (first, middle, last) against the FP64 oracle."""
+    m, n, batch = 1000, 300, 486
+    rng = np.random.default_rng(486)
+    X = (rng.standard_normal((batch, m, n)) + 1j * rng.standard_normal((batch, m, n))).astype(np.complex64)
+    U = rng.standard_normal((batch, m, 8)) + 1j * rng.standard_normal((batch, m, 8))
+    V = rng.standard_normal((batch, 8, n)) + 1j * rng.standard_normal((batch, 8, n))
+    X += (4.0 * np.einsum("bij,bjk->bik", U, V)).astype(np.complex64)
+    betas = [40.0 + (b % 7) for b in range(batch)]
+    cm = np.ascontiguousarray(np.transpose(X, (0, 2, 1)))
+    from mslr_recon_b200.context import FORMS
+    out = M.svst_batch(dev(torch, cm), m, n, betas, form=FORMS[form]).cpu().numpy()
+    out = np.transpose(out, (0, 2, 1))
+    for b in (0, batch // 2, batch - 1):
+        ref = O.svst(X[b].astype(np.complex128), betas[b])
+        assert rel(out[b], ref) < SVST_TOL[form], (b, rel(out[b], ref))
+
+
 def test_svst_single_matrix(torch, M):
     rng = np.random.default_rng(12)
     X = (rng.standard_normal((50, 20)) + 1j * rng.standard_normal((50, 20))).astype(np.complex64)
