@@ -55,6 +55,7 @@ static void free_ctx(mslr_ctx* c) {
   if (c->gev_out) cudaEventDestroy(c->gev_out);
   if (c->gstream) cudaStreamDestroy(c->gstream);
   if (c->d_nuc) cudaFree(c->d_nuc);
+  if (c->d_dft) cudaFree(c->d_dft);
   if (c->d_zero) cudaFree(c->d_zero);
   if (c->d_cost_g) cudaFree(c->d_cost_g);
   if (c->d_cost_part) cudaFree(c->d_cost_part);

@@ -101,7 +101,14 @@ int dc_cost_eval(Ctx* c, const cf* X, int ns, double* dc_out, cudaStream_t st) {
   const int64_t E = (int64_t)c->Nt * c->nvox;
   if (!c->d_cost_g && (rc = dalloc(c, (void**)&c->d_cost_g, (size_t)E * sizeof(cf)))) return rc;
   if ((rc = ensure_part(c))) return rc;
-  if ((rc = normal_op(c, X, ns, E, c->d_cost_g, true, st))) return rc;
+  // the cost is a difference of terms ~‖y‖² that cancel as the iterate
+  // converges: evaluate it with the FP32 FFT plane pass, not the split-BF16
+  // tensor-core one
+  const bool tc = c->xy_tc;
+  c->xy_tc = false;
+  rc = normal_op(c, X, ns, E, c->d_cost_g, true, st);
+  c->xy_tc = tc;
+  if (rc) return rc;
   k_cost_dots<<<kBlocks, kThreads, 0, st>>>(X, ns, E, c->d_cost_g, c->d_ahy, E, c->d_cost_part);
   MSLR_CUDA_TRY(cudaGetLastError());
   c->launches += 1;

@@ -78,6 +78,8 @@ struct Ctx {
   bool spec = false;      // shape-specialised kernels (sense_spec.cu) exist for N
   int spec_xy_ctas = 0;   // resident CTAs of the specialised plane kernel
   int spec_zfwd_ctas = 0; // resident CTAs of the specialised forward z kernel
+  bool xy_tc = false;     // tensor-core plane pass (DFT products on tcgen05)
+  uint32_t* d_dft = nullptr;   // its split-BF16 DFT matrix tiles
   // graph-captured POGM step (tuned form): captured on a private stream the
   // first time pogm_step sees a given X, replayed afterwards
   cudaStream_t gstream = nullptr;

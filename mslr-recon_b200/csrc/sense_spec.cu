@@ -23,9 +23,16 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
 
 #include "fft_spec.cuh"
 #include "internal.h"
+#include "umma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -364,6 +371,278 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, 2)
 }
 
 // ---------------------------------------------------------------------------
+// Tensor-core plane pass (tcgen05).  The four 1-D transforms of a plane are
+// dense DFT products on the tensor cores: with F[n][k] = e^{−2πi nk/N} (zero
+// padded to NP, a multiple of 16) and the plane P[y][x] (y rows),
+//   D1 = P F          (x forward;   A = P,    K-major, rows y)
+//   D2ᵀ = D1ᵀ F       (y forward;   A = D1ᵀ,  MN-major, rows kx)
+//   D3ᵀ = (M ⊙ D2)ᵀ F̄ (mask, y inverse; A K-major, rows kx)
+//   D4 = D3 F̄         (x inverse;   A = D3,   MN-major, rows y)
+// each a complex GEMM of M=128 × N=NP × K=NP on planar split-BF16 operands
+// (hi·hi + hi·lo + lo·hi for each of the four real products; the conjugate of
+// F through the negate bit), accumulated in TMEM (real and imaginary halves).
+// Between products every thread takes its TMEM lane (a row of the result),
+// splits it into BF16 hi / lo and writes it as the next A operand — in the
+// K-major or the MN-major core-matrix layout, so no transposes are needed.
+// F lives in shared memory for the whole kernel; one CTA per SM, persistent
+// over the planes of the chunk.
+template <int N>
+struct XyT {
+  static_assert(N % 2 == 0, "pairs of columns move as 16-byte vectors");
+  static constexpr int NP = (N + 31) / 32 * 32;   // padded DFT length (two column halves of 16s)
+  static constexpr int KC = NP / 8;               // 8-element cores per 8-row group
+  static constexpr int AW = 128 * NP / 2;         // 32-bit words of a 128 × NP bf16 tile
+  static constexpr int FW = NP * NP / 2;          // words of an NP × NP tile
+  static constexpr unsigned SBO = KC * 128;
+  static constexpr unsigned COLS = 256;           // TMEM columns: re [0, NP), im [NP, 2 NP)
+  static_assert(2 * NP <= (int)COLS, "two accumulators must fit the allocation");
+};
+
+template <int N, int MW>
+struct XyUSmem {
+  uint32_t F[4][XyT<N>::FW];   // Fr_h, Fr_l, Fi_h, Fi_l   (K-major, row n, column k)
+  uint32_t A[4][XyT<N>::AW];   // Ar_h, Ar_l, Ai_h, Ai_l
+  uint32_t mask[MW];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+// element offset (bf16) of the first of 8 consecutive K elements (K-major) or
+// 8 consecutive M elements (MN-major) of a tile with KC cores per row group
+template <int KC>
+__device__ __forceinline__ int kmaj8(int m, int k) { return ((m >> 3) * KC + (k >> 3)) * 64 + (m & 7) * 8; }
+template <int KC>
+__device__ __forceinline__ int mnmaj8(int mn, int k) { return ((mn >> 3) * KC + (k >> 3)) * 64 + (k & 7) * 8; }
+
+// 8 complex values → 16 bytes in each of the four planar hi / lo tiles
+__device__ __forceinline__ void put8(uint32_t* const* A, int eoff, const float* re, const float* im) {
+  uint4 rh, rl, ih, il;
+  umma::split_pair(re[0], re[1], rh.x, rl.x);
+  umma::split_pair(re[2], re[3], rh.y, rl.y);
+  umma::split_pair(re[4], re[5], rh.z, rl.z);
+  umma::split_pair(re[6], re[7], rh.w, rl.w);
+  umma::split_pair(im[0], im[1], ih.x, il.x);
+  umma::split_pair(im[2], im[3], ih.y, il.y);
+  umma::split_pair(im[4], im[5], ih.z, il.z);
+  umma::split_pair(im[6], im[7], ih.w, il.w);
+  const int w = eoff >> 1;
+  *reinterpret_cast<uint4*>(A[0] + w) = rh;
+  *reinterpret_cast<uint4*>(A[1] + w) = rl;
+  *reinterpret_cast<uint4*>(A[2] + w) = ih;
+  *reinterpret_cast<uint4*>(A[3] + w) = il;
+}
+
+// one complex DFT product into TMEM (issued by one thread): A (MN-major when
+// AMN) times F (forward) or conj(F) (INV)
+template <int N, int MW, bool AMN, bool INV>
+__device__ __forceinline__ void dft_gemm(const XyUSmem<N, MW>& s, uint32_t dre, uint32_t dim) {
+  using X = XyT<N>;
+  constexpr uint32_t P = umma::idesc(128, X::NP, false, false, AMN, false);
+  constexpr uint32_t Ng = umma::idesc(128, X::NP, true, false, AMN, false);
+#pragma unroll 1
+  for (int t = 0; t < X::NP / 16; ++t) {
+    auto a = [&](int i) { return umma::sdesc(s.A[i] + t * 64, 128, X::SBO); };
+    auto f = [&](int i) { return umma::sdesc(s.F[i] + t * 64, 128, X::SBO); };
+    const bool acc = t > 0;
+    // Re += Ar·Fr ∓ Ai·Fi      (forward: −, inverse: +)
+    umma::mma(dre, a(0), f(0), P, acc);
+    umma::mma(dre, a(0), f(1), P, true);
+    umma::mma(dre, a(1), f(0), P, true);
+    umma::mma(dre, a(2), f(2), INV ? P : Ng, true);
+    umma::mma(dre, a(2), f(3), INV ? P : Ng, true);
+    umma::mma(dre, a(3), f(2), INV ? P : Ng, true);
+    // Im += ±Ar·Fi + Ai·Fr     (forward: +, inverse: −)
+    umma::mma(dim, a(0), f(2), INV ? Ng : P, acc);
+    umma::mma(dim, a(0), f(3), INV ? Ng : P, true);
+    umma::mma(dim, a(1), f(2), INV ? Ng : P, true);
+    umma::mma(dim, a(2), f(0), P, true);
+    umma::mma(dim, a(2), f(1), P, true);
+    umma::mma(dim, a(3), f(0), P, true);
+  }
+}
+
+template <class Sh>
+__global__ void __launch_bounds__(256, 1)
+    k_xy_umma(cf* __restrict__ T, const uint32_t* __restrict__ mask, int nwords, int t0, int nf,
+              int Nc, const uint32_t* __restrict__ Fg, int* __restrict__ err) {
+  static_assert(Sh::NX == Sh::NY, "square planes");
+  constexpr int N = Sh::NX, NZ = Sh::NZ, PL = Sh::PL, MW = Sh::MW;
+  constexpr int64_t NVOX = Sh::NVOX;
+  using X = XyT<N>;
+  using Sm = XyUSmem<N, MW>;
+  constexpr int NP = X::NP, KC = X::KC;
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  Sm& s = *reinterpret_cast<Sm*>(smraw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int row = (warp & 3) * 32 + lane;   // TMEM lane of this thread
+  const int half = warp >> 2;              // column half of the epilogues
+  // DFT matrix into shared memory, operand tile cleared (rows >= NP stay zero)
+  for (int i = tid; i < 4 * X::FW / 4; i += 256)
+    reinterpret_cast<uint4*>(&s.F[0][0])[i] = __ldg(reinterpret_cast<const uint4*>(Fg) + i);
+  for (int i = tid; i < 4 * X::AW / 4; i += 256)
+    reinterpret_cast<uint4*>(&s.A[0][0])[i] = make_uint4(0u, 0u, 0u, 0u);
+  umma::tmem_alloc(&s.tmem, X::COLS);
+  if (tid == 0) {
+    umma::mbar_init(&s.bar);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  umma::fence_after();
+  const uint32_t tm = s.tmem;
+  const uint32_t lane_addr = tm + ((uint32_t)((warp & 3) * 32) << 16);
+  uint32_t* Aarr[4] = {s.A[0], s.A[1], s.A[2], s.A[3]};
+  const int units = NZ * Nc * nf;
+  unsigned phase = 0;
+  bool ok = true;
+  // one GEMM: make the operand visible, issue, wait; false on time-out
+  auto run = [&](auto amn, auto inv) {
+    umma::fence_async_smem();
+    umma::fence_before();
+    __syncthreads();
+    if (tid == 0 && ok) {
+      umma::fence_after();
+      dft_gemm<N, MW, decltype(amn)::value, decltype(inv)::value>(s, tm, tm + NP);
+      umma::commit(&s.bar);
+    }
+    if (ok && !umma::mbar_wait(&s.bar, phase)) ok = false;
+    phase ^= 1u;
+    ok = __syncthreads_and(ok);
+    umma::fence_after();
+  };
+  using F_ = std::false_type;
+  using T_ = std::true_type;
+  for (int u = blockIdx.x; u < units && ok; u += gridDim.x) {
+    const int kz = u % NZ, r = u / NZ;
+    const int c = r % Nc, ff = r / Nc;
+    cf* pl = T + ((int64_t)ff * Nc + c) * NVOX + (int64_t)kz * PL;
+    const int64_t bit0 = (int64_t)kz * PL;
+    const int w0 = (int)(bit0 >> 5);
+    const int moff = (int)(bit0 - (int64_t)w0 * 32);
+    const uint32_t* mrow = mask + (int64_t)(t0 + ff) * nwords;
+    for (int i = tid; i < MW; i += 256) s.mask[i] = (w0 + i < nwords) ? __ldg(mrow + w0 + i) : 0u;
+    // E0: plane rows → A (K-major, m = y, k = x)
+    if (row < NP) {
+      for (int cb = 0; cb < NP / 32; ++cb) {
+        const int c0 = half * (NP / 2) + cb * 16;
+        float re[16], im[16];
+#pragma unroll
+        for (int j = 0; j < 16; j += 2) {
+          const int x = c0 + j;
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (row < N && x < N) v = __ldg(reinterpret_cast<const float4*>(pl + row * N + x));
+          re[j] = v.x;
+          im[j] = v.y;
+          re[j + 1] = v.z;
+          im[j + 1] = v.w;
+        }
+        put8(Aarr, kmaj8<KC>(row, c0), re, im);
+        put8(Aarr, kmaj8<KC>(row, c0 + 8), re + 8, im + 8);
+      }
+    }
+    run(F_{}, F_{});   // D1 = P F: lanes y, columns kx
+    // E1: D1 → A (MN-major, mn = kx, k = y)
+    for (int cb = 0; cb < NP / 32; ++cb) {
+      const int c0 = half * (NP / 2) + cb * 16;
+      float re[16], im[16];
+      umma::ld16(lane_addr + c0, re);
+      umma::ld16(lane_addr + NP + c0, im);
+      if (row < NP) {
+        put8(Aarr, mnmaj8<KC>(c0, row), re, im);
+        put8(Aarr, mnmaj8<KC>(c0 + 8, row), re + 8, im + 8);
+      }
+    }
+    run(T_{}, F_{});   // D2ᵀ: lanes kx, columns ky
+    // E2: mask, → A (K-major, m = kx, k = ky)
+    for (int cb = 0; cb < NP / 32; ++cb) {
+      const int c0 = half * (NP / 2) + cb * 16;
+      float re[16], im[16];
+      umma::ld16(lane_addr + c0, re);
+      umma::ld16(lane_addr + NP + c0, im);
+      if (row < NP) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int ky = c0 + j;
+          bool keep = false;
+          if (row < N && ky < N) {
+            const int b = moff + ky * N + row;
+            keep = (s.mask[b >> 5] >> (b & 31)) & 1u;
+          }
+          if (!keep) re[j] = im[j] = 0.f;
+        }
+        put8(Aarr, kmaj8<KC>(row, c0), re, im);
+        put8(Aarr, kmaj8<KC>(row, c0 + 8), re + 8, im + 8);
+      }
+    }
+    run(F_{}, T_{});   // D3ᵀ: lanes kx, columns y
+    // E3: → A (MN-major, mn = y, k = kx)
+    for (int cb = 0; cb < NP / 32; ++cb) {
+      const int c0 = half * (NP / 2) + cb * 16;
+      float re[16], im[16];
+      umma::ld16(lane_addr + c0, re);
+      umma::ld16(lane_addr + NP + c0, im);
+      if (row < NP) {
+        put8(Aarr, mnmaj8<KC>(c0, row), re, im);
+        put8(Aarr, mnmaj8<KC>(c0 + 8, row), re + 8, im + 8);
+      }
+    }
+    run(T_{}, T_{});   // D4: lanes y, columns x
+    // E4: → plane rows in global memory
+    for (int cb = 0; cb < NP / 32; ++cb) {
+      const int c0 = half * (NP / 2) + cb * 16;
+      float re[16], im[16];
+      umma::ld16(lane_addr + c0, re);
+      umma::ld16(lane_addr + NP + c0, im);
+      if (row < N) {
+#pragma unroll
+        for (int j = 0; j < 16; j += 2) {
+          const int x = c0 + j;
+          if (x < N) *reinterpret_cast<float4*>(pl + row * N + x) = make_float4(re[j], im[j], re[j + 1], im[j + 1]);
+        }
+      }
+    }
+    umma::fence_before();
+    __syncthreads();   // plane done: A and the mask words may be rewritten
+  }
+  if (__syncthreads_or(!ok) && tid == 0) atomicOr(err, kErrWait);
+  umma::tmem_free(tm, X::COLS);
+}
+
+// F[n][k] = e^{−2πi nk/N}, zero padded to NP × NP, as the four split-BF16
+// K-major tiles of k_xy_umma (host, double precision before the split)
+template <int N>
+std::vector<uint32_t> dft_tiles() {
+  using X = XyT<N>;
+  constexpr int NP = X::NP, KC = X::KC;
+  std::vector<uint16_t> t(4 * (size_t)NP * NP, 0);
+  auto bf = [](float v) {   // round to nearest even
+    uint32_t b;
+    std::memcpy(&b, &v, 4);
+    return (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);
+  };
+  auto fl = [](uint16_t h) {
+    const uint32_t b = (uint32_t)h << 16;
+    float v;
+    std::memcpy(&v, &b, 4);
+    return v;
+  };
+  for (int n = 0; n < N; ++n)
+    for (int k = 0; k < N; ++k) {
+      const double a = -2.0 * 3.14159265358979323846 * (double)((int64_t)n * k % N) / N;
+      const float re = (float)std::cos(a), im = (float)std::sin(a);
+      const uint16_t rh = bf(re), ih = bf(im);
+      const uint16_t rl = bf(re - fl(rh)), il = bf(im - fl(ih));
+      const size_t e = (size_t)((n >> 3) * KC + (k >> 3)) * 64 + (n & 7) * 8 + (k & 7);
+      t[0 * (size_t)NP * NP + e] = rh;
+      t[1 * (size_t)NP * NP + e] = rl;
+      t[2 * (size_t)NP * NP + e] = ih;
+      t[3 * (size_t)NP * NP + e] = il;
+    }
+  std::vector<uint32_t> w(t.size() / 2);
+  std::memcpy(w.data(), t.data(), t.size() * sizeof(uint16_t));
+  return w;
+}
+
+// ---------------------------------------------------------------------------
 struct SpecOps {
   int nx, ny, nz;
   const void* zfwd;
@@ -371,22 +650,34 @@ struct SpecOps {
   const void* zadj;
   int zfwd_threads, xy_threads, zadj_threads;
   size_t smem_zfwd, smem_zadj, smem_xy;
+  const void* xy_tc;                       // tensor-core plane pass (square planes), or null
+  size_t smem_xy_tc;
+  std::vector<uint32_t> (*dft)();          // its DFT tiles
 };
 
 template <class Sh>
 SpecOps ops_of() {
-  return SpecOps{Sh::NX,
-                 Sh::NY,
-                 Sh::NZ,
-                 reinterpret_cast<const void*>(&k_zfwd4<Sh>),
-                 reinterpret_cast<const void*>(&k_xy3<Sh>),
-                 reinterpret_cast<const void*>(&k_zadj5<Sh>),
-                 Sh::ZW * 32,
-                 Sh::XYW * 32,
-                 Sh::ZW2 * 32,
-                 Sh::smem_zfwd,
-                 Sh::smem_zadj,
-                 Sh::smem_xy};
+  SpecOps o{Sh::NX,
+            Sh::NY,
+            Sh::NZ,
+            reinterpret_cast<const void*>(&k_zfwd4<Sh>),
+            reinterpret_cast<const void*>(&k_xy3<Sh>),
+            reinterpret_cast<const void*>(&k_zadj5<Sh>),
+            Sh::ZW * 32,
+            Sh::XYW * 32,
+            Sh::ZW2 * 32,
+            Sh::smem_zfwd,
+            Sh::smem_zadj,
+            Sh::smem_xy,
+            nullptr,
+            0,
+            nullptr};
+  if constexpr (Sh::NX == Sh::NY && Sh::NX <= 128) {
+    o.xy_tc = reinterpret_cast<const void*>(&k_xy_umma<Sh>);
+    o.smem_xy_tc = sizeof(XyUSmem<Sh::NX, Sh::MW>);
+    o.dft = &dft_tiles<Sh::NX>;
+  }
+  return o;
 }
 
 // Compiled shapes: the reference's fMRI volume (90×90×60) and smaller cubes
@@ -429,6 +720,21 @@ bool sense_spec_setup(Ctx* c) {
   cudaGetLastError();
   c->spec_xy_ctas = per_sm * c->nsm;
   c->spec_zfwd_ctas = per_sm_z * c->nsm;
+  // tensor-core plane pass only on request (MSLR_XY_PATH=tc): at 90×90 its
+  // padded split-BF16 DFT products (12 MMAs of 128×96×16 per K step, four
+  // products per plane, serialised with their epilogues) take longer than the
+  // FP32 FFT plane pass
+  const char* xp = std::getenv("MSLR_XY_PATH");
+  c->xy_tc = false;
+  if (o->xy_tc && xp && std::string(xp) == "tc" && o->smem_xy_tc <= 227 * 1024 &&
+      !cudaFuncSetAttribute(o->xy_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)o->smem_xy_tc)) {
+    const std::vector<uint32_t> t = o->dft();
+    if (!c->d_dft && !dalloc(c, (void**)&c->d_dft, t.size() * sizeof(uint32_t)) &&
+        !cudaMemcpy(c->d_dft, t.data(), t.size() * sizeof(uint32_t), cudaMemcpyHostToDevice))
+      c->xy_tc = true;
+  }
+  cudaGetLastError();
   return true;
 }
 
@@ -475,7 +781,14 @@ int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
                                        o->smem_zfwd, st));
       }
       if (int rc = prof_mark(c, st)) return rc;
-      {
+      if (c->xy_tc) {
+        const int units = Nz * ch * f;
+        const int grid = std::max(1, std::min(units, c->nsm));
+        const uint32_t* dft = c->d_dft;
+        void* args[] = {(void*)&T,  (void*)&mask, (void*)&nwords, (void*)&t0, (void*)&f,
+                        (void*)&ch, (void*)&dft,  (void*)&err};
+        MSLR_CUDA_TRY(cudaLaunchKernel(o->xy_tc, dim3(grid), dim3(256), args, o->smem_xy_tc, st));
+      } else {
         const int units = Nz * ch * f;
         const int grid = std::max(1, std::min(units, c->spec_xy_ctas));
         void* args[] = {(void*)&T,  (void*)&mask,       (void*)&nwords,      (void*)&t0, (void*)&f,

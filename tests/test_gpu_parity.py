@@ -75,6 +75,7 @@ def test_recombine_matches_reference_order(torch, M, N, ps, ss):
 
 # --- SVST ------------------------------------------------------------------------
 SVST_TOL = {"plain": 2e-5, "tuned": 1e-4}   # FP32 SIMT; split-precision BF16x3 tensor cores
+NORMAL_TOL = {"plain": 1e-5, "tuned": 1e-5, "tuned-tc": 5e-5}   # FP32 FFTs; split-BF16 tensor-core plane DFTs
 
 
 @pytest.mark.parametrize("form", ["plain", "tuned"])
@@ -295,6 +296,7 @@ def test_state_errors(torch, M, gold):
 def test_sense_metric_shapes(torch, M, form, N, Nc):
     """Forward, adjoint and normal operator at the benchmark image shapes
     (two-pass radix plans in the tuned kernels; an odd axis included)."""
+    ctx_form = "tuned" if form.startswith("tuned") else form
     rng = np.random.default_rng(sum(N) + Nc)
     Nx, Ny, Nz = N
     Nt = 3
@@ -305,7 +307,7 @@ def test_sense_metric_shapes(torch, M, form, N, Nc):
     idx = np.stack([np.sort(rng.choice(nvox, K, replace=False)) for _ in range(Nt)]).astype(np.int32)
     x = rng.standard_normal((Nt, Nz, Ny, Nx)) + 1j * rng.standard_normal((Nt, Nz, Ny, Nx))
     y = rng.standard_normal((Nt, Nc, K)) + 1j * rng.standard_normal((Nt, Nc, K))
-    with M.MSLRContext(N, Nc, Nt, K, [[Nx, Ny, Nz]], [[Nx, Ny, Nz]], form=form) as ctx:
+    with M.MSLRContext(N, Nc, Nt, K, [[Nx, Ny, Nz]], [[Nx, Ny, Nz]], form=ctx_form) as ctx:
         ctx.bind(dev(torch, smaps), dev(torch, y), dev(torch, idx, torch.int32))
         yf = ctx.forward(dev(torch, x)).cpu().numpy()
         assert rel(yf, O.sense_forward(x, smaps, idx)) < 1e-5
@@ -313,4 +315,12 @@ def test_sense_metric_shapes(torch, M, form, N, Nc):
         assert rel(xa, O.sense_adjoint(y, smaps, idx)) < 1e-5
         g = ctx.normal(dev(torch, x[None])).cpu().numpy()
         ref = O.sense_adjoint(O.sense_forward(x, smaps, idx) - y, smaps, idx)
-        assert rel(g, ref) < 1e-5
+        assert rel(g, ref) < NORMAL_TOL[form], rel(g, ref)
+
+
+def test_normal_op_tensor_core_plane_pass(torch, M, monkeypatch):
+    """The optional plane pass of the tuned normal operator as tcgen05 DFT
+    products (MSLR_XY_PATH=tc) at 90×90×60: within 5e-5 of the FP64 oracle
+    (split-BF16 products), and the POGM-facing forward / adjoint unchanged."""
+    monkeypatch.setenv("MSLR_XY_PATH", "tc")
+    test_sense_metric_shapes(torch, M, "tuned-tc", (90, 90, 60), 18)
