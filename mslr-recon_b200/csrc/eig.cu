@@ -42,6 +42,7 @@ namespace {
 constexpr int kT = 1024;   // most threads per CTA (one row / eigenvalue per thread)
 constexpr int kSmallT = 384;   // CTA size for n <= 384: two patches share an SM
 constexpr int kNb = 16;    // reflectors per WY block
+constexpr int kCW = 16;    // eigenvectors per back-transform pass
 
 __device__ __forceinline__ float warp_sum(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -107,6 +108,7 @@ struct EigArgs {
   Seg seg[kMaxSeg];
   const double* thr;   // device: threshold scale (ζ or β), or per patch
   int thr_per_patch;
+  int rz;              // eigenvectors staged in shared memory (more: global slots)
 };
 
 // vectors are padded to n + 32 entries (zero tails) so 32-wide tiles read them in bounds
@@ -117,12 +119,39 @@ size_t part_bytes(int n) {
   return T * (T + 1) / 2 * 64 * sizeof(cf);
 }
 
-size_t smem_bytes(int n, int threads) {
+size_t vec_bytes(int n) {
   const size_t np = (size_t)n + 32;
-  const size_t vecs = 3 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
-                      3 * (size_t)n * sizeof(float) + 64 * sizeof(float) + 64 * sizeof(double);
-  const size_t wy = (size_t)n * kNb * sizeof(cf) + 2 * kNb * kNb * sizeof(cf);
-  return vecs + std::max(wy, threads <= kSmallT ? part_bytes(n) : (size_t)0) + 128;
+  return 3 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) + 3 * (size_t)n * sizeof(float) +
+         64 * sizeof(float) + 64 * sizeof(double);
+}
+
+// Buffers of the back-transform besides the vector stage: Y (n × kNb), T and
+// YᴴY (kNb × kNb each), S and T·S (kNb × kCW each), one partial sum per thread.
+size_t wy_bytes(int n, int threads) {
+  return ((size_t)n * kNb + 2 * kNb * kNb + 2 * kNb * kCW + (size_t)threads) * sizeof(cf);
+}
+
+// The region after the vectors, by phase: the matvec partial sums (phase 1,
+// 384-thread variant), the FP64 twisted-factorisation columns of up to rz
+// eigenvectors (phase 3: z and D+, n × rz doubles each), the complex
+// eigenvector stage (n × rz) followed by the back-transform buffers (phase 4).
+size_t smem_bytes(int n, int threads, int rz) {
+  const size_t stage = (size_t)n * rz * sizeof(cf);
+  size_t region = std::max(2 * stage, stage + wy_bytes(n, threads));
+  if (threads <= kSmallT) region = std::max(region, part_bytes(n));
+  return vec_bytes(n) + region + 128;
+}
+
+// Dynamic shared memory one CTA may use: two CTAs per SM for the 384-thread
+// variant (228 KB per SM, 1 KB reserved per CTA), one for the large variant;
+// both leave room for the kernel's static shared variables.
+size_t smem_budget(int threads) { return threads <= kSmallT ? 112 * 1024 : 227 * 1024 - 1024; }
+
+// eigenvectors staged in shared memory: the most that fit beside everything else
+int stage_cols(int n, int threads) {
+  int rz = 0;
+  while (rz < n && smem_bytes(n, threads, rz + 1) <= smem_budget(threads)) ++rz;
+  return rz;
 }
 
 template <int MAXT, int MINB>
@@ -359,7 +388,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   }
   __syncthreads();
 
-  // ---- 2. eigenvalues above β² (FP64 bisection, thread per eigenvalue) -------
+  // ---- 2. eigenvalues above β² (FP64 multisection) ----------------------------
   if (tid == 0) {
     double gl = dd[0], gu = dd[0], emax2 = 0.0;
     for (int q = 0; q < n; ++q) {
@@ -385,19 +414,49 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   const double gl = fmax(s_bd[0], beta_d * beta_d), gu = s_bd[1], pivmin = s_bd[2],
                tnorm = s_bd[3];
   if (tid == 0) S.rank[ip] = r;
-  if (tid < r) {
-    const int kth = n - 1 - tid;   // tid-th largest = kth smallest
-    double lo = gl, hi = gu;
-    for (int it = 0; it < 80; ++it) {
-      const double mid = 0.5 * (lo + hi);
-      if (mid <= lo || mid >= hi) break;
-      if (sturm_less(dd, ee2, n, mid, pivmin) > kth) hi = mid;
-      else lo = mid;
+  {
+    // A group of gsz threads (a power of two, at most a warp) per eigenvalue:
+    // each round counts the eigenvalues below gsz evenly spaced interior
+    // points of the bracket and keeps the sub-interval holding the
+    // eigenvalue, a factor gsz + 1 per round of Sturm sequences instead of
+    // bisection's 2.
+    int gsz = 1;
+    while (gsz < 32 && 2 * gsz * r <= kT) gsz <<= 1;
+    const int e = tid / gsz, sl = tid & (gsz - 1);
+    if (warp * 32 < r * gsz) {   // whole warps, for the shuffles
+      const int kth = n - 1 - e;   // e-th largest = kth smallest
+      const double frac = (double)(sl + 1) / (double)(gsz + 1);
+      double lo = gl, hi = gu;
+      bool done = e >= r;
+      for (int it = 0; it < 200; ++it) {
+        if (!__any_sync(0xffffffffu, !done)) break;
+        const double x = lo + (hi - lo) * frac;
+        const bool ok = !done && x > lo && x < hi;
+        const bool up = ok && sturm_less(dd, ee2, n, x, pivmin) > kth;   // eigenvalue below x
+        double nlo = (ok && !up) ? x : lo;
+        double nhi = (ok && up) ? x : hi;
+        int any = ok ? 1 : 0;
+        for (int o = 1; o < gsz; o <<= 1) {
+          nlo = fmax(nlo, __shfl_xor_sync(0xffffffffu, nlo, o));
+          nhi = fmin(nhi, __shfl_xor_sync(0xffffffffu, nhi, o));
+          any |= __shfl_xor_sync(0xffffffffu, any, o);
+        }
+        if (!done) {
+          if (!any || !(nlo < nhi)) {
+            done = true;
+          } else {
+            lo = nlo;
+            hi = nhi;
+          }
+        }
+      }
+      if (e < r && sl == 0) {
+        const double lm = 0.5 * (lo + hi);
+        lam[e] = lm;
+        const double sg = sqrt(fmax(lm, 0.0));
+        hv[e] = (sg > beta_d && sg > 0.0) ? (float)((sg - beta_d) / sg) : 0.f;
+      }
     }
-    const double lm = 0.5 * (lo + hi);
-    lam[tid] = lm;
-    const double sg = sqrt(fmax(lm, 0.0));
-    hv[tid] = (sg > beta_d && sg > 0.0) ? (float)((sg - beta_d) / sg) : 0.f;
   }
   __syncthreads();
   if (S.nuc) {   // nuclear norm of the patch (src/recon.jl:138-146): Σ σ_i = Σ √λ_i
@@ -411,31 +470,38 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     return;
   }
 
+  // Up to g.rz eigenvectors live in shared memory from here to the output
+  // ([row][vector], row stride rz); more use the patch's global slots (row
+  // stride n).  zb / zs address them either way.
+  const bool stg = r <= g.rz;
+  const int64_t zs = stg ? g.rz : n;
+  cf* zb = stg ? sY : Z;
+
   // ---- 3. eigenvectors of T (FP64 twisted factorisation) --------------------
-  // D+ in AUX[j][i]; D− and then z_j in the Z slot [j][i] read as a double;
-  // finally converted in place to complex float.
+  // z_j in the vector slots read as doubles, D+ after them (shared) or in
+  // AUX (global); finally converted in place to complex float.
   if (tid < r) {
     const double lm = lam[tid];
-    double* dp = AUX + tid;
-    double* zd = reinterpret_cast<double*>(Z) + tid;
+    double* zd = reinterpret_cast<double*>(zb) + tid;
+    double* dp = (stg ? reinterpret_cast<double*>(zb) + (int64_t)n * zs : AUX) + tid;
     double q = dd[0] - lm;
     if (fabs(q) < pivmin) q = -pivmin;
     dp[0] = q;
     for (int j = 0; j + 1 < n; ++j) {
       q = dd[j + 1] - lm - ee2[j] / q;
       if (fabs(q) < pivmin) q = -pivmin;
-      dp[(int64_t)(j + 1) * n] = q;
+      dp[(int64_t)(j + 1) * zs] = q;
     }
     q = dd[n - 1] - lm;
     if (fabs(q) < pivmin) q = -pivmin;
-    zd[(int64_t)(n - 1) * n] = q;
+    zd[(int64_t)(n - 1) * zs] = q;
     int kb = n - 1;
-    double gb = fabs(dp[(int64_t)(n - 1) * n] + q - (dd[n - 1] - lm));
+    double gb = fabs(dp[(int64_t)(n - 1) * zs] + q - (dd[n - 1] - lm));
     for (int j = n - 2; j >= 0; --j) {
       q = dd[j] - lm - ee2[j] / q;
       if (fabs(q) < pivmin) q = -pivmin;
-      zd[(int64_t)j * n] = q;
-      const double gm = fabs(dp[(int64_t)j * n] + q - (dd[j] - lm));
+      zd[(int64_t)j * zs] = q;
+      const double gm = fabs(dp[(int64_t)j * zs] + q - (dd[j] - lm));
       if (gm < gb) {
         gb = gm;
         kb = j;
@@ -443,22 +509,22 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     }
     double nrm = 1.0, zp = 1.0;
     for (int j = kb - 1; j >= 0; --j) {   // z_j = −e_j z_{j+1} / D+_j
-      zp = -ee[j] * zp / dp[(int64_t)j * n];
-      zd[(int64_t)j * n] = zp;
+      zp = -ee[j] * zp / dp[(int64_t)j * zs];
+      zd[(int64_t)j * zs] = zp;
       nrm += zp * zp;
     }
-    zd[(int64_t)kb * n] = 1.0;
+    zd[(int64_t)kb * zs] = 1.0;
     zp = 1.0;
     for (int j = kb + 1; j < n; ++j) {    // z_j = −e_{j−1} z_{j−1} / D−_j
-      zp = -ee[j - 1] * zp / zd[(int64_t)j * n];
-      zd[(int64_t)j * n] = zp;
+      zp = -ee[j - 1] * zp / zd[(int64_t)j * zs];
+      zd[(int64_t)j * zs] = zp;
       nrm += zp * zp;
     }
     const double inv = 1.0 / sqrt(nrm);
-    cf* zc = Z + tid;
+    cf* zc = zb + tid;
     for (int j = 0; j < n; ++j) {
-      const double zj = zd[(int64_t)j * n];
-      zc[(int64_t)j * n] = make_float2((float)(zj * inv), 0.f);
+      const double zj = zd[(int64_t)j * zs];
+      zc[(int64_t)j * zs] = make_float2((float)(zj * inv), 0.f);
     }
   }
   __syncthreads();
@@ -475,22 +541,22 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
         for (int attempt = 0; attempt < 4; ++attempt) {
           for (int pv = s0; pv < qv; ++pv) {
             double dot = 0.0;
-            for (int j = tid; j < n; j += kT) dot += (double)Z[(int64_t)j * n + pv].x * Z[(int64_t)j * n + qv].x;
+            for (int j = tid; j < n; j += kT) dot += (double)zb[j * zs + pv].x * zb[j * zs + qv].x;
             dot = block_sum_d(dot, redd + 32 * (rb++ & 1));
-            for (int j = tid; j < n; j += kT) Z[(int64_t)j * n + qv].x -= (float)dot * Z[(int64_t)j * n + pv].x;
+            for (int j = tid; j < n; j += kT) zb[j * zs + qv].x -= (float)dot * zb[j * zs + pv].x;
             __syncthreads();
           }
           double nr = 0.0;
-          for (int j = tid; j < n; j += kT) nr += (double)Z[(int64_t)j * n + qv].x * Z[(int64_t)j * n + qv].x;
+          for (int j = tid; j < n; j += kT) nr += (double)zb[j * zs + qv].x * zb[j * zs + qv].x;
           nr = sqrt(block_sum_d(nr, redd + 32 * (rb++ & 1)));
           if (nr > 0.1) {
-            for (int j = tid; j < n; j += kT) Z[(int64_t)j * n + qv].x /= (float)nr;
+            for (int j = tid; j < n; j += kT) zb[j * zs + qv].x /= (float)nr;
             __syncthreads();
             break;
           }
           // collapsed onto earlier vectors: restart from a unit vector
           for (int j = tid; j < n; j += kT)
-            Z[(int64_t)j * n + qv].x = (j == (qv + attempt * 7919) % n) ? 1.f : 0.f;
+            zb[j * zs + qv].x = (j == (qv + attempt * 7919) % n) ? 1.f : 0.f;
           __syncthreads();
         }
       }
@@ -499,8 +565,17 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   }
 
   // ---- 4. V = H_0 ⋯ H_{n-2} Z, blocks of kNb reflectors from the last ---------
-  cf* sT = sY + (int64_t)n * kNb;   // kNb × kNb, T[a][b] at a*kNb + b
-  cf* sYY = sT + kNb * kNb;         // Yᴴ Y
+  // Staged vectors (few): every thread takes part — S = Yᴴ Z by (output, row
+  // group) partial sums added in a fixed order, S ← T S, then Z −= Y S by
+  // (row, vector) element, in passes of kCW vectors.  Vectors in global
+  // memory (many): thread i updates vector i with its block coefficients in
+  // registers.
+  cf* sYb = sY + (int64_t)n * g.rz;   // Y: n × kNb, [row][reflector], after the vector stage
+  cf* sT = sYb + (int64_t)n * kNb;    // kNb × kNb, T[a][b] at a*kNb + b
+  cf* sYY = sT + kNb * kNb;           // Yᴴ Y
+  cf* sS = sYY + kNb * kNb;           // kNb × kCW
+  cf* sS2 = sS + kNb * kCW;           // T S
+  cf* sP = sS2 + kNb * kCW;           // partial sums, one per thread
   const int nref = n - 1;
   for (int kend = nref; kend > 0; kend -= kNb) {
     const int k0 = max(0, kend - kNb);
@@ -513,14 +588,14 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
         if (row == k + 1) y = make_float2(1.f, 0.f);
         else if (row > k + 1) y = A[(int64_t)k * n + row];
       }
-      sY[q] = y;
+      sYb[q] = y;
     }
     __syncthreads();
     if (tid < kNb * kNb) {   // Yᴴ Y
       const int a = tid / kNb, b = tid - a * kNb;
       float sr = 0.f, si = 0.f;
       for (int row = k0 + 1; row < n; ++row) {
-        const cf ya = sY[row * kNb + a], yb = sY[row * kNb + b];
+        const cf ya = sYb[row * kNb + a], yb = sYb[row * kNb + b];
         sr += ya.x * yb.x + ya.y * yb.y;
         si += ya.x * yb.y - ya.y * yb.x;
       }
@@ -543,57 +618,109 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
       }
     }
     __syncthreads();
-    if (tid < r) {   // vector tid: S = Yᴴ z;  S ← T S;  z −= Y S
-      cf Sv[kNb];
+    if (!stg) {   // vectors in global memory: thread tid updates vector tid (S = Yᴴ z; S ← T S; z −= Y S)
+      if (tid < r) {
+        cf Sv[kNb];
 #pragma unroll
-      for (int jj = 0; jj < kNb; ++jj) Sv[jj] = make_float2(0.f, 0.f);
-      for (int row = k0 + 1; row < n; ++row) {
-        const cf z = Z[(int64_t)row * n + tid];
+        for (int jj = 0; jj < kNb; ++jj) Sv[jj] = make_float2(0.f, 0.f);
+        for (int row = k0 + 1; row < n; ++row) {
+          const cf z = Z[(int64_t)row * n + tid];
 #pragma unroll
-        for (int jj = 0; jj < kNb; ++jj) {
-          const cf y = sY[row * kNb + jj];   // conj(y)·z
-          Sv[jj].x += y.x * z.x + y.y * z.y;
-          Sv[jj].y += y.x * z.y - y.y * z.x;
+          for (int jj = 0; jj < kNb; ++jj) {
+            const cf y = sYb[row * kNb + jj];   // conj(y)·z
+            Sv[jj].x += y.x * z.x + y.y * z.y;
+            Sv[jj].y += y.x * z.y - y.y * z.x;
+          }
+        }
+        // T upper-triangular: S[a] is last needed by row a itself (in place)
+#pragma unroll
+        for (int a = 0; a < kNb; ++a) {
+          cf sacc = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int b = a; b < kNb; ++b) sacc = cadd(sacc, cmul(sT[a * kNb + b], Sv[b]));
+          Sv[a] = sacc;
+        }
+        constexpr int kB = 8;   // rows per batch: loads issued before stores
+        int row = k0 + 1;
+        for (; row + kB <= n; row += kB) {
+          cf z[kB];
+#pragma unroll
+          for (int b = 0; b < kB; ++b) z[b] = __ldcg(Z + (int64_t)(row + b) * n + tid);
+#pragma unroll
+          for (int b = 0; b < kB; ++b) {
+#pragma unroll
+            for (int jj = 0; jj < kNb; ++jj) z[b] = csub(z[b], cmul(sYb[(row + b) * kNb + jj], Sv[jj]));
+          }
+#pragma unroll
+          for (int b = 0; b < kB; ++b) Z[(int64_t)(row + b) * n + tid] = z[b];
+        }
+        for (; row < n; ++row) {
+          cf z = Z[(int64_t)row * n + tid];
+#pragma unroll
+          for (int jj = 0; jj < kNb; ++jj) z = csub(z, cmul(sYb[row * kNb + jj], Sv[jj]));
+          Z[(int64_t)row * n + tid] = z;
         }
       }
-      // T upper-triangular: S[a] is last needed by row a itself (in place)
-#pragma unroll
-      for (int a = 0; a < kNb; ++a) {
-        cf sacc = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int b = a; b < kNb; ++b) sacc = cadd(sacc, cmul(sT[a * kNb + b], Sv[b]));
-        Sv[a] = sacc;
-      }
-      constexpr int kB = 8;   // rows per batch: loads issued before stores
-      int row = k0 + 1;
-      for (; row + kB <= n; row += kB) {
-        cf z[kB];
-#pragma unroll
-        for (int b = 0; b < kB; ++b) z[b] = __ldcg(Z + (int64_t)(row + b) * n + tid);
-#pragma unroll
-        for (int b = 0; b < kB; ++b) {
-#pragma unroll
-          for (int jj = 0; jj < kNb; ++jj) z[b] = csub(z[b], cmul(sY[(row + b) * kNb + jj], Sv[jj]));
-        }
-#pragma unroll
-        for (int b = 0; b < kB; ++b) Z[(int64_t)(row + b) * n + tid] = z[b];
-      }
-      for (; row < n; ++row) {
-        cf z = Z[(int64_t)row * n + tid];
-#pragma unroll
-        for (int jj = 0; jj < kNb; ++jj) z = csub(z, cmul(sY[row * kNb + jj], Sv[jj]));
-        Z[(int64_t)row * n + tid] = z;
-      }
+      __syncthreads();
+      continue;
     }
-    __syncthreads();
+    // vectors staged in shared memory: every thread takes part
+    for (int c0 = 0; c0 < r; c0 += kCW) {
+      const int cw = min(kCW, r - c0);
+      const int no = kNb * cw;   // outputs of S = Yᴴ Z (at most 256 <= threads)
+      const int ng = kT / no;    // row groups
+      if (tid < no * ng) {
+        const int o = tid % no, grp = tid / no;
+        const int jj = o / cw, c = c0 + (o - jj * cw);
+        float sr = 0.f, si = 0.f;
+        for (int row = k0 + 1 + grp; row < n; row += ng) {
+          const cf y = sYb[row * kNb + jj], z = zb[row * zs + c];   // conj(y)·z
+          sr += y.x * z.x + y.y * z.y;
+          si += y.x * z.y - y.y * z.x;
+        }
+        sP[tid] = make_float2(sr, si);
+      }
+      __syncthreads();
+      if (tid < no) {
+        float sr = 0.f, si = 0.f;
+        for (int gq = 0; gq < ng; ++gq) {
+          sr += sP[gq * no + tid].x;
+          si += sP[gq * no + tid].y;
+        }
+        sS[tid] = make_float2(sr, si);
+      }
+      __syncthreads();
+      if (tid < no) {   // T upper-triangular
+        const int a = tid / cw, c = tid - a * cw;
+        cf sacc = make_float2(0.f, 0.f);
+        for (int b = a; b < kNb; ++b) sacc = cadd(sacc, cmul(sT[a * kNb + b], sS[b * cw + c]));
+        sS2[tid] = sacc;
+      }
+      __syncthreads();
+      const int rows = n - (k0 + 1);
+      for (int q = tid; q < rows * cw; q += kT) {
+        const int rr = q / cw, c = q - rr * cw;
+        const int row = k0 + 1 + rr;
+        cf* zp = zb + row * zs + c0 + c;
+        cf z = *zp;
+#pragma unroll
+        for (int jj = 0; jj < kNb; ++jj) z = csub(z, cmul(sYb[row * kNb + jj], sS2[jj * cw + c]));
+        *zp = z;
+      }
+      __syncthreads();
+    }
   }
 
   // ---- 5. Ṽ = conj(V) diag(√h), columns >= r zero ------------------------------
-  for (int c = tid; c < n; c += kT) {
-    const float sh = (c < r) ? sqrtf(hv[c]) : 0.f;
-    for (int row = 0; row < n; ++row) {
-      const cf z = (c < r) ? Z[(int64_t)row * n + c] : make_float2(0.f, 0.f);
-      Z[(int64_t)row * n + c] = make_float2(z.x * sh, -z.y * sh);
+  for (int row = 0; row < n; ++row) {
+    for (int c = tid; c < n; c += kT) {
+      cf v = make_float2(0.f, 0.f);
+      if (c < r) {
+        const cf z = zb[row * zs + c];
+        const float sh = sqrtf(hv[c]);
+        v = make_float2(z.x * sh, -z.y * sh);
+      }
+      Z[(int64_t)row * n + c] = v;
     }
   }
 }
@@ -602,12 +729,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
 
 int eig2_prepare(int nmax) {
   if (nmax > kT) return fail(MSLR_ERR_UNSUPPORTED, "Gram side above 1024");
-  const size_t sm = smem_bytes(nmax, kT);
-  if (sm > 227 * 1024) return fail(MSLR_ERR_UNSUPPORTED, "Gram side too large for the eigen stage");
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  if (nmax <= kSmallT)
-    MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem_bytes(nmax, kSmallT)));
+  if (smem_bytes(nmax, kT, 0) > smem_budget(kT))
+    return fail(MSLR_ERR_UNSUPPORTED, "Gram side too large for the eigen stage");
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_budget(kT)));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem_budget(kSmallT)));
   return MSLR_OK;
 }
 
@@ -634,10 +761,13 @@ int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int th
     total += segs[s].np;
     nmax = std::max(nmax, segs[s].n);
   }
-  if (nmax <= kSmallT)
-    k_eig<kSmallT, 2><<<(unsigned)total, kSmallT, smem_bytes(nmax, kSmallT), st>>>(a);
+  const int threads = nmax <= kSmallT ? kSmallT : kT;
+  a.rz = stage_cols(nmax, threads);
+  const size_t sm = smem_bytes(nmax, threads, a.rz);
+  if (threads == kSmallT)
+    k_eig<kSmallT, 2><<<(unsigned)total, kSmallT, sm, st>>>(a);
   else
-    k_eig<kT, 1><<<(unsigned)total, kT, smem_bytes(nmax, kT), st>>>(a);
+    k_eig<kT, 1><<<(unsigned)total, kT, sm, st>>>(a);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
 }
