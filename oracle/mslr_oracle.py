@@ -491,3 +491,148 @@ def rel_err(a: np.ndarray, b: np.ndarray) -> float:
     b = np.asarray(b, dtype=np.complex128)
     nb = float(np.linalg.norm(b))
     return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
+
+
+# ---------------------------------------------------------------------------
+# Differentiation of the unrolled POGM with respect to log λ_k.
+#
+# The reference does not differentiate run_recon; this section restates the
+# forward it does run (pogm_mod with mom=:pogm, restart=:gr and run_recon's
+# aliasing g_prox, src/mirt_mod.jl:74-188, scripts/reconstruct.jl:196-202) as
+# the explicit recurrence that aliasing reduces it to
+#     u_i = x_{i-1} − α ∇f(x_{i-1})
+#     z_i = (1 + β_i + γ_i) u_i − β_i u_{i-1} − γ_i x_{i-1},   u_0 = x_0
+#     x_i = prox_{ζ_i}(z_i)       (per scale: patch SVST, threshold ζ_i λ_k)
+# with the restart decisions and momentum scalars of the run held fixed
+# (they are piecewise constant in λ), and differentiates
+#     loss = ½ ‖Σ_k X_k − X_true‖²
+# by reverse accumulation.  The patch-SVST backward uses the Gram form of
+# SVST: for a patch matrix A (p × q, p ≥ q; otherwise applied to Aᴴ),
+#     Y = A W,  W = f(G) = V f(Λ) Vᴴ,  G = Aᴴ A,  f(λ) = max(1 − β/√λ, 0),
+#     Ā = Ȳ W + A K,   K = V (F ⊙ Vᴴ (W̄ + W̄ᴴ) V) Vᴴ,   W̄ = Aᴴ Ȳ,
+#     ∂loss/∂β = Σ_i ∂f/∂β(λ_i) Re (Vᴴ W̄ V)_ii,
+# F the divided differences of f (Daleckii–Krein).
+# ---------------------------------------------------------------------------
+def svst_divided_differences(lam: np.ndarray, beta: float):
+    """(f(λ), ∂f/∂β(λ), F) for f(λ) = max(1 − β/√λ, 0) at the eigenvalues
+    ``lam`` of a patch Gram matrix; F_ij = (f_i − f_j)/(λ_i − λ_j), f'(λ_i) on
+    the diagonal, written without cancellation."""
+    s = np.sqrt(np.maximum(lam, 0.0))
+    above = s > beta
+    f = np.where(above, 1.0 - beta / np.where(above, s, 1.0), 0.0)
+    fb = np.where(above, -1.0 / np.where(above, s, 1.0), 0.0)
+    si, sj = s[:, None], s[None, :]
+    ai, aj = above[:, None], above[None, :]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        both = beta / (si * sj * (si + sj))
+        i_only = (si - beta) / (si * (si - sj) * (si + sj))
+        j_only = (sj - beta) / (sj * (sj - si) * (si + sj))
+    F = np.where(ai & aj, both, np.where(ai & ~aj, i_only, np.where(~ai & aj, j_only, 0.0)))
+    return f, fb, F
+
+
+def svst_vjp(A: np.ndarray, beta: float, Ybar: np.ndarray):
+    """Cotangent of A and of β for Y = SVST(A, β) (src/recon.jl:183-211),
+    given the cotangent Ybar of Y (real inner product Re tr(Xᴴ Y))."""
+    if A.shape[0] < A.shape[1]:
+        Abar, bb = svst_vjp(A.conj().T, beta, Ybar.conj().T)
+        return Abar.conj().T, bb
+    G = A.conj().T @ A
+    lam, V = np.linalg.eigh(G)
+    f, fb, F = svst_divided_differences(lam, beta)
+    W = (V * f) @ V.conj().T
+    Wbar = A.conj().T @ Ybar
+    D = V.conj().T @ Wbar @ V
+    K = V @ (F * (D + D.conj().T)) @ V.conj().T
+    return Ybar @ W + A @ K, float(np.sum(fb * D.real.diagonal()))
+
+
+def patch_svst_vjp(img: np.ndarray, beta: float, img_bar: np.ndarray, patch_size, stride_size):
+    """Cotangent of ``patch_svst(img, β, ...)`` (src/recon.jl:251-256) with
+    respect to img and β.  img2patches is a gather and patches2img a
+    coverage-weighted sum, so their adjoints are a weighted gather and a
+    scatter-add."""
+    Nt, Nz, Ny, Nx = img.shape
+    cnt = np.maximum(coverage_count((Nx, Ny, Nz), patch_size, stride_size), 1.0)
+    P = img2patches(img, patch_size, stride_size)
+    Pb = img2patches(img_bar / cnt[None], patch_size, stride_size)
+    out = np.zeros_like(P)
+    bsum = 0.0
+    for ip in range(P.shape[0]):
+        a, bb = svst_vjp(P[ip].T, beta, Pb[ip].T)
+        out[ip] = a.T
+        bsum += bb
+    return patches2img(out, patch_size, stride_size, (Nx, Ny, Nz)) * cnt[None], bsum
+
+
+def pogm_unrolled(prob: ReconProblem, niter: int, lambdas=None, L: float | None = None,
+                  restart_cutoff: float = 0.0, bsig: float = 1.0, dtype=np.complex128):
+    """Forward of the unrolled POGM from X0 = A'y (scripts/reconstruct.jl:209-226)
+    with per-scale weights ``lambdas``.  Returns (X_niter, tape, restarts);
+    tape[i] = (z_i, α, β_i, γ_i, ζ_i)."""
+    Nx, Ny, Nz = prob.N
+    Nt, Ns = prob.Nt, prob.Ns
+    lam = list(prob.lambdas() if lambdas is None else lambdas)
+    L = prob.lipschitz() if L is None else L
+    smaps, y, idx, w = prob.smaps.astype(dtype), prob.y.astype(dtype), prob.idx, prob.workers
+    x = np.zeros((Ns, Nt, Nz, Ny, Nx), dtype=dtype)
+    x[0] = sense_adjoint(y, smaps, idx, w)
+    u_old = x.copy()
+    alpha = 1.0 / L
+    t, sig = 1.0, 1.0
+    gold = np.zeros_like(x)
+    tape, restarts = [], [False]
+    for it in range(1, niter + 1):
+        g = sense_adjoint(sense_forward(x.sum(axis=0), smaps, idx, w) - y, smaps, idx, w)
+        G = np.broadcast_to(g[None], x.shape)
+        u = x - alpha * G
+        tnew = 0.5 * (1 + math.sqrt(1 + (8 if it == niter else 4) * t * t))
+        beta = (t - 1) / tnew
+        gamma = sig * t / tnew
+        z = u + beta * (u - u_old) + gamma * (u - x)
+        zeta = alpha * (1 + beta + gamma)
+        xn = np.empty_like(z)
+        for k in range(Ns):
+            xn[k] = patch_svst(z[k], zeta * lam[k], prob.patch_sizes[k], prob.strides[k])
+        tape.append((z, alpha, beta, gamma, zeta))
+        rs = _gr_restart(G, u - u_old, restart_cutoff)
+        if rs:
+            tnew, sig = 1.0, 1.0
+        elif float(np.sum(np.real(G * gold), dtype=np.float64)) < 0:
+            sig = bsig * sig
+        restarts.append(bool(rs))
+        gold = np.array(G)
+        u_old, x, t = u, xn, tnew
+    return x, tape, restarts
+
+
+def unrolled_loss(X: np.ndarray, X_true: np.ndarray) -> float:
+    """½ ‖Σ_k X_k − X_true‖² (FP64 sum)."""
+    r = X.sum(axis=0).astype(np.complex128) - X_true
+    return 0.5 * float(np.vdot(r, r).real)
+
+
+def pogm_unrolled_grad(prob: ReconProblem, niter: int, X_true: np.ndarray, lambdas=None,
+                       L: float | None = None, restart_cutoff: float = 0.0, bsig: float = 1.0):
+    """loss and ∂loss/∂log λ_k of the unrolled POGM by reverse accumulation
+    through the stored z_i (the eigen-decompositions are recomputed)."""
+    lam = list(prob.lambdas() if lambdas is None else lambdas)
+    X, tape, restarts = pogm_unrolled(prob, niter, lam, L, restart_cutoff, bsig)
+    smaps, idx, w = prob.smaps.astype(np.complex128), prob.idx, prob.workers
+    Ns = prob.Ns
+    r = X.sum(axis=0) - X_true
+    loss = 0.5 * float(np.vdot(r, r).real)
+    xbar = np.broadcast_to(r[None], X.shape).copy()
+    ubar = np.zeros_like(X)
+    grad = np.zeros(Ns)
+    for z, alpha, beta, gamma, zeta in reversed(tape):
+        zbar = np.empty_like(z)
+        for k in range(Ns):
+            thr = zeta * lam[k]
+            zbar[k], bb = patch_svst_vjp(z[k], thr, xbar[k], prob.patch_sizes[k], prob.strides[k])
+            grad[k] += thr * bb
+        wv = ubar + (1 + beta + gamma) * zbar
+        hw = normal_op(wv.sum(axis=0), smaps, idx, w)
+        xbar = wv - alpha * hw[None] - gamma * zbar
+        ubar = -beta * zbar
+    return loss, grad, X, restarts
