@@ -204,6 +204,52 @@ int mslr_set_graph(mslr_ctx* ctx, int32_t enable);
 /* Restart flags of the iterations run so far (host array of niter+1). */
 int mslr_pogm_restarts(mslr_ctx* ctx, uint8_t* restarts_host, void* stream);
 
+/* Set-up of run_recon's inputs on the device (scripts/reconstruct.jl:86-147).
+ *
+ * mslr_sos_normalize: smaps_out = S ./ (sqrt.(sum(abs2.(S); dims=4)) .+ eps(Float32))
+ *   for raw coil maps S (Nx,Ny,Nz,Nc) (:89), Float32, coils summed in order.
+ *   smaps_out may equal smaps_raw.
+ * mslr_sampling: the sampling mask Ω = ksp[:,:,:,1,:] .!= 0 of the zero-filled
+ *   k-space ksp (Nx,Ny,Nz,Nc,Nt) and the checks of :109-118 — every coil has
+ *   coil 1's pattern, every frame the same count (MSLR_ERR_ARG with the
+ *   reference's messages otherwise).  *K receives the samples per frame; with
+ *   idx / y non-NULL (capacity K_cap per frame) it also gathers the 0-based
+ *   ascending indices idx (K, Nt) and the samples y (K, Nc, Nt) (:144-147).
+ * mslr_prepare: on a context created with that K — normalised maps into
+ *   smaps_out, idx and the samples gathered, bound, then the scale factor
+ *   quantile(abs.(sense_comb(ksp, smaps)), 0.99) (:100-104, src/recon.jl:310-321;
+ *   type-7 quantile, exact order statistics) into *scale_factor, y divided by
+ *   max(scale, eps(Float32)) in place and the context bound to it.  The mask
+ *   is taken before the division; a sample that the division turns into zero
+ *   is reported as MSLR_ERR_ARG.  Synchronises `stream`. */
+int mslr_sos_normalize(const int32_t N[3], int32_t Nc, const void* smaps_raw, void* smaps_out,
+                       void* stream);
+int mslr_sampling(const int32_t N[3], int32_t Nc, int32_t Nt, const void* ksp, int64_t* K, int32_t* idx,
+                  void* y, int64_t K_cap, void* stream);
+int mslr_prepare(mslr_ctx* ctx, const void* ksp, const void* smaps_raw, void* smaps_out, void* y_out,
+                 int32_t* idx_out, double* scale_factor, void* stream);
+
+/* Per-scale regularisation weights λ_k (scripts/reconstruct.jl:164-169 computes
+ * them by the Ong–Lustig formula; mslr_create starts from those values).
+ * The threshold of scale k in g_prox is ζ·λ_k (scripts/reconstruct.jl:196-202). */
+int mslr_set_lambdas(mslr_ctx* ctx, const double* lambdas);
+int mslr_get_lambdas(const mslr_ctx* ctx, double* lambdas);
+
+/* Gradient of the unrolled POGM.  Runs niter iterations of mslr_pogm_run's
+ * recurrence from X0 = A'y (scripts/reconstruct.jl:209-226; X receives
+ * x_niter) and returns loss = ½‖Σ_k X[..,k] − X_true‖² (X_true
+ * (Nx,Ny,Nz,Nt), FP64 sum) and grad_loglam[k] = d loss / d log λ_k, by
+ * reverse accumulation through the SENSE normal operator and the patch-SVST
+ * backward, with z_i stored per iteration and each patch's eigen-
+ * decomposition recomputed.  Restart decisions and momentum scalars are held
+ * at their values in this run (the loss is piecewise smooth in λ).  No
+ * counterpart in the reference, which does not differentiate run_recon.
+ * Allocates its checkpoints (niter × Ns images) on first use.  Synchronises
+ * `stream`. */
+int mslr_pogm_grad(mslr_ctx* ctx, const void* X_true, int32_t niter, double L, double restart_cutoff,
+                   double bsig, void* X, double* loss, double* grad_loglam, uint8_t* restarts_host,
+                   void* stream);
+
 /* Number of kernels this context has launched so far (host-side count). */
 int mslr_launch_count(const mslr_ctx* ctx, uint64_t* count);
 

@@ -47,6 +47,22 @@ def ong_lustig_lambdas(N, Nt, patch_sizes):
     return out
 
 
+def sampling(ksp: torch.Tensor, idx=None, y=None, stream=None) -> int:
+    """Samples per frame K of the zero-filled k-space ksp (Nt, Nc, Nz, Ny, Nx)
+    — Ω from coil 1 with the checks of scripts/reconstruct.jl:109-118
+    (ValueError with the reference's message otherwise); with idx (Nt, K)
+    int32 and y (Nt, Nc, K) given, also gathers them (:144-147)."""
+    if ksp.dim() != 5 or ksp.dtype != torch.complex64 or not ksp.is_cuda or not ksp.is_contiguous():
+        raise ValueError("ksp must be a contiguous complex64 CUDA tensor (Nt, Nc, Nz, Ny, Nx)")
+    Nt, Nc, Nz, Ny, Nx = ksp.shape
+    K = C.c_int64()
+    cap = idx.shape[1] if idx is not None else 0
+    check(lib.mslr_sampling(i32arr([Nx, Ny, Nz]), Nc, Nt, ksp.data_ptr(), C.byref(K),
+                            idx.data_ptr() if idx is not None else None,
+                            y.data_ptr() if y is not None else None, cap, _stream_ptr(stream)))
+    return int(K.value)
+
+
 class MSLRContext:
     """One reconstruction context.
 
@@ -218,6 +234,48 @@ class MSLRContext:
         r = (C.c_uint8 * (self._niter + 1))()
         self._chk(lib.mslr_pogm_restarts(self._h, r, _stream_ptr(stream)))
         return [bool(v) for v in r]
+
+    def prepare(self, ksp: torch.Tensor, smaps_raw: torch.Tensor, stream=None):
+        """scripts/reconstruct.jl:86-147 on the device from the zero-filled
+        k-space ksp (Nt, Nc, Nz, Ny, Nx) and raw coil maps (Nc, Nz, Ny, Nx):
+        SOS-normalised maps, Ω and its checks, the samples y / indices idx,
+        the scale factor quantile(|sense_comb|, 0.99), y scaled; the context
+        is bound.  Returns (smaps, y, idx, scale_factor)."""
+        _dev_c64(ksp, (self.Nt, self.Nc) + self.img_shape[1:], "ksp")
+        _dev_c64(smaps_raw, (self.Nc,) + self.img_shape[1:], "smaps_raw")
+        dev = ksp.device
+        smaps = torch.empty_like(smaps_raw)
+        y = torch.empty((self.Nt, self.Nc, self.K), dtype=torch.complex64, device=dev)
+        idx = torch.empty((self.Nt, self.K), dtype=torch.int32, device=dev)
+        sf = C.c_double()
+        self._chk(lib.mslr_prepare(self._h, ksp.data_ptr(), smaps_raw.data_ptr(), smaps.data_ptr(),
+                                   y.data_ptr(), idx.data_ptr(), C.byref(sf), _stream_ptr(stream)))
+        return smaps, y, idx, float(sf.value)
+
+    def set_lambdas(self, lambdas):
+        """Per-scale weights λ_k of g_prox (scripts/reconstruct.jl:164-169, 196-202)."""
+        lam = [float(v) for v in lambdas]
+        if len(lam) != self.Ns:
+            raise ValueError(f"need {self.Ns} lambdas")
+        self._chk(lib.mslr_set_lambdas(self._h, (C.c_double * self.Ns)(*lam)))
+        self.lambdas = lam
+
+    def pogm_grad(self, X_true: torch.Tensor, niter: int, L: float, restart_cutoff: float = 0.0,
+                  bsig: float = 1.0, X=None, stream=None):
+        """Unrolled POGM from X0 = A'y and its gradient: returns (loss,
+        d loss/d log λ_k per scale, X_niter, restart flags) for
+        loss = ½‖Σ_k X_k − X_true‖²; X_true is (Nt, Nz, Ny, Nx)."""
+        _dev_c64(X_true, self.img_shape, "X_true")
+        if X is None:
+            X = torch.empty(self.x_shape, dtype=torch.complex64, device=X_true.device)
+        _dev_c64(X, self.x_shape, "X")
+        loss = C.c_double()
+        grad = (C.c_double * self.Ns)()
+        r = (C.c_uint8 * (niter + 1))()
+        self._chk(lib.mslr_pogm_grad(self._h, X_true.data_ptr(), int(niter), float(L),
+                                     float(restart_cutoff), float(bsig), X.data_ptr(), C.byref(loss),
+                                     grad, r, _stream_ptr(stream)))
+        return float(loss.value), [float(g) for g in grad], X, [bool(v) for v in r]
 
     def launch_count(self) -> int:
         n = C.c_uint64()

@@ -2,6 +2,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <string>
+
 #include "internal.h"
 #include "patchmap.cuh"
 
@@ -59,6 +61,9 @@ static void free_ctx(mslr_ctx* c) {
   if (c->d_zero) cudaFree(c->d_zero);
   if (c->d_cost_g) cudaFree(c->d_cost_g);
   if (c->d_cost_part) cudaFree(c->d_cost_part);
+  if (c->d_ckpt) cudaFree(c->d_ckpt);
+  if (c->d_gbuf) cudaFree(c->d_gbuf);
+  if (c->d_vjpw) cudaFree(c->d_vjpw);
   delete c;
 }
 
@@ -386,6 +391,84 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
   }
+  int32_t herr = 0;
+  cudaError_t e = cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
+  if (herr & 4)
+    return ctx_fail(ctx, fail(MSLR_ERR_NONFINITE, "non-finite value in the POGM restart sums"));
+  if (herr & 8)
+    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a device-side wait for a bulk copy timed out"));
+  int uerr = 0;
+  CTX_RET(ctx, umma_take_error(&uerr));
+  if (uerr)
+    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a tensor-core kernel's wait for its MMAs timed out"));
+  return MSLR_OK;
+}
+
+int mslr_sos_normalize(const int32_t N[3], int32_t Nc, const void* smaps_raw, void* smaps_out,
+                       void* stream) {
+  if (!N || !smaps_raw || !smaps_out || Nc <= 0 || N[0] <= 0 || N[1] <= 0 || N[2] <= 0)
+    return fail(MSLR_ERR_ARG, "bad argument");
+  const int n3[3] = {N[0], N[1], N[2]};
+  return sos_normalize(n3, Nc, reinterpret_cast<const cf*>(smaps_raw), reinterpret_cast<cf*>(smaps_out),
+                       reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mslr_sampling(const int32_t N[3], int32_t Nc, int32_t Nt, const void* ksp, int64_t* K, int32_t* idx,
+                  void* y, int64_t K_cap, void* stream) {
+  if (!N || !ksp || !K || Nc <= 0 || Nt <= 0 || N[0] <= 0 || N[1] <= 0 || N[2] <= 0)
+    return fail(MSLR_ERR_ARG, "bad argument");
+  const int n3[3] = {N[0], N[1], N[2]};
+  return sampling(n3, Nc, Nt, reinterpret_cast<const cf*>(ksp), K, idx, reinterpret_cast<cf*>(y), K_cap,
+                  reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mslr_prepare(mslr_ctx* ctx, const void* ksp, const void* smaps_raw, void* smaps_out, void* y_out,
+                 int32_t* idx_out, double* scale_factor, void* stream) {
+  CTX_CHECK(ctx);
+  if (!ksp || !smaps_raw || !smaps_out || !y_out || !idx_out || !scale_factor)
+    return ctx_fail(ctx, fail(MSLR_ERR_ARG, "null argument"));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cf* smaps = reinterpret_cast<cf*>(smaps_out);
+  cf* y = reinterpret_cast<cf*>(y_out);
+  CTX_RET(ctx, sos_normalize(ctx->N, ctx->Nc, reinterpret_cast<const cf*>(smaps_raw), smaps, st));
+  int64_t K = 0;
+  CTX_RET(ctx, sampling(ctx->N, ctx->Nc, ctx->Nt, reinterpret_cast<const cf*>(ksp), &K, idx_out, y,
+                        ctx->K, st));
+  if (K != ctx->K)
+    return ctx_fail(ctx, fail(MSLR_ERR_ARG, "the k-space has " + std::to_string(K) +
+                                                " samples per frame, the context " +
+                                                std::to_string(ctx->K)));
+  CTX_RET(ctx, sense_bind(ctx, smaps, y, idx_out, 0, st));
+  CTX_RET(ctx, prepare_scale(ctx, smaps, y, idx_out, scale_factor, st));
+  return MSLR_OK;
+}
+
+int mslr_set_lambdas(mslr_ctx* ctx, const double* lambdas) {
+  CTX_CHECK(ctx);
+  if (!lambdas) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "null argument"));
+  CTX_RET(ctx, set_lambdas(ctx, lambdas));
+  return MSLR_OK;
+}
+
+int mslr_get_lambdas(const mslr_ctx* ctx, double* lambdas) {
+  CTX_CHECK(ctx);
+  if (!lambdas) return fail(MSLR_ERR_ARG, "null argument");
+  for (int k = 0; k < ctx->Ns; ++k) lambdas[k] = ctx->lambdas[k];
+  return MSLR_OK;
+}
+
+int mslr_pogm_grad(mslr_ctx* ctx, const void* X_true, int32_t niter, double L, double restart_cutoff,
+                   double bsig, void* X, double* loss, double* grad_loglam, uint8_t* restarts_host,
+                   void* stream) {
+  CTX_CHECK(ctx);
+  NEED_BOUND(ctx);
+  if (!X_true || !X || !loss || !grad_loglam) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "null argument"));
+  CTX_RET(ctx, check_pogm_args(ctx, niter, L, restart_cutoff, bsig));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  CTX_RET(ctx, pogm_grad(ctx, reinterpret_cast<const cf*>(X_true), niter, L, restart_cutoff, bsig,
+                         reinterpret_cast<cf*>(X), loss, grad_loglam, restarts_host, st));
   int32_t herr = 0;
   cudaError_t e = cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -99,6 +99,7 @@ struct Seg {
   int* rank;       // np
   double lam;      // threshold multiplier of the segment (λ_k)
   double* nuc;     // values-only mode when set: np sums Σ √λ_i over λ_i above β², no vectors
+  double* lam_out; // full mode when set: all n eigenpairs, V unscaled in zv, λ (descending) here
 };
 
 constexpr int kMaxSeg = 8;
@@ -188,7 +189,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   __shared__ double s_bd[4];
   __shared__ int s_r;
 
-  const double beta_d = g.thr[g.thr_per_patch ? (int64_t)blockIdx.x : 0] * S.lam;
+  const bool full = S.lam_out != nullptr;
+  const double beta_d = full ? 0.0 : g.thr[g.thr_per_patch ? (int64_t)blockIdx.x : 0] * S.lam;
   const float beta = (float)beta_d;
   (void)beta;
 
@@ -407,12 +409,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     s_bd[2] = pivmin;
     s_bd[3] = tnorm;
     const double thr2 = beta_d * beta_d;
-    s_r = (thr2 >= gu) ? 0 : n - sturm_less(dd, ee2, n, thr2, pivmin);
+    s_r = full ? n : (thr2 >= gu) ? 0 : n - sturm_less(dd, ee2, n, thr2, pivmin);
   }
   __syncthreads();
   const int r = s_r;
-  const double gl = fmax(s_bd[0], beta_d * beta_d), gu = s_bd[1], pivmin = s_bd[2],
-               tnorm = s_bd[3];
+  const double gl = full ? s_bd[0] : fmax(s_bd[0], beta_d * beta_d), gu = s_bd[1],
+               pivmin = s_bd[2], tnorm = s_bd[3];
   if (tid == 0) S.rank[ip] = r;
   {
     // A group of gsz threads (a power of two, at most a warp) per eigenvalue:
@@ -712,6 +714,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   }
 
   // ---- 5. Ṽ = conj(V) diag(√h), columns >= r zero ------------------------------
+  if (full) {   // V itself and the eigenvalues
+    for (int c = tid; c < n; c += kT) S.lam_out[ip * n + c] = lam[c];
+    for (int row = 0; row < n; ++row)
+      for (int c = tid; c < n; c += kT) Z[(int64_t)row * n + c] = zb[row * zs + c];
+    return;
+  }
   for (int row = 0; row < n; ++row) {
     for (int c = tid; c < n; c += kT) {
       cf v = make_float2(0.f, 0.f);
@@ -758,6 +766,7 @@ int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int th
     S.rank = segs[s].rank;
     S.lam = segs[s].lam;
     S.nuc = segs[s].nuc;
+    S.lam_out = segs[s].lam_out;
     total += segs[s].np;
     nmax = std::max(nmax, segs[s].n);
   }

@@ -65,6 +65,13 @@ struct Ctx {
   double* d_zero = nullptr;    // device 0.0 (threshold of the values-only eigen mode)
   cf* d_cost_g = nullptr;      // gradient scratch of the cost evaluation (Nt, nvox)
   double* d_cost_part = nullptr;   // FP64 block partials of the cost inner products
+  // unrolled-POGM gradient (grad.cu): z_i of every iteration, the adjoint
+  // state (x̄, ū, z̄, w, A'A w, scratch image) and the patch-SVST backward
+  cf* d_ckpt = nullptr;
+  int grad_ckpt_cap = 0;
+  cf* d_gbuf = nullptr;
+  void* d_vjpw = nullptr;
+  size_t vjpw_bytes = 0;
   cf* d_T = nullptr;           // (F, Nc, nvox) per-coil k-space of a chunk of frames
   int F = 1;
   bool bound = false;
@@ -165,6 +172,8 @@ struct EigSegment {
   int* rank;     // np
   double lam;
   double* nuc = nullptr;   // when set: per-patch Σ √λ above the threshold only (no vectors, no W)
+  double* lam_out = nullptr;   // when set: every eigenpair — V (row-major, G = V Λ Vᴴ) in zv
+                               // and the eigenvalues (descending, np × n) here; threshold unused
 };
 int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int thr_per_patch,
                      cudaStream_t st);
@@ -184,5 +193,29 @@ int pogm_step(Ctx* c, cf* X, cudaStream_t st);
 int init_x0(Ctx* c, cf* X, cudaStream_t st);
 int power_iter(Ctx* c, int niter, double tol, double* sigma1, int* iters, cudaStream_t st);
 int set_scalar(double* dst, double v, cudaStream_t st);
+
+// ---- set-up of run_recon's inputs (setup.cu) ---------------------------------
+int sos_normalize(const int N[3], int Nc, const cf* in, cf* out, cudaStream_t st);
+int sampling(const int N[3], int Nc, int Nt, const cf* ksp, int64_t* K, int32_t* idx, cf* y,
+             int64_t K_cap, cudaStream_t st);
+int prepare_scale(Ctx* c, const cf* smaps, cf* y, const int32_t* idx, double* scale_out, cudaStream_t st);
+
+// ---- unrolled-POGM gradient (grad.cu; patch-SVST backward in svst.cu) ---------
+struct PatchMap;
+int set_lambdas(Ctx* c, const double* lam);
+int pogm_grad(Ctx* c, const cf* Xtrue, int niter, double L, double cutoff, double bsig, cf* X,
+              double* loss, double* grad, uint8_t* restarts_h, cudaStream_t st);
+int svst_vjp_setup(Ctx* c);
+int svst_vjp_scale(Ctx* c, int s, const cf* z, const cf* xbar, double beta, cf* zbar, cf* tmp,
+                   double* bbar, cudaStream_t st);
+int xgram_launch(const cf* imgO, const cf* imgM, const PatchMap& m, int64_t np, cf* out, cf* part,
+                 int nsplit, cudaStream_t st);
+int bgemm_launch(int opa, int opb, const cf* A, const cf* B, cf* C, int n, int64_t np, cudaStream_t st);
+int divdiff_launch(const cf* D, const double* lam, const cf* V, double beta, int n, int64_t np, cf* E,
+                   cf* T3, double* bbar, cudaStream_t st);
+int vjp_rebuild_launch(const cf* xb, const cf* z, const cf* W, const cf* K, const PatchMap& m,
+                       int64_t np, cf* out, int direct, cudaStream_t st);
+int div_count_launch(const cf* img, const PatchMap& m, const int* cover, cf* out, cudaStream_t st);
+int patch_sum_launch(const cf* P, const PatchMap& m, const int* cover, cf* img, cudaStream_t st);
 
 }  // namespace mslr

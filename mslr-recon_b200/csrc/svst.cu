@@ -379,7 +379,10 @@ int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
   return svst_rebuild(in, m, np, w, out, direct, tc, st, launches);
 }
 
+// Split-K partial Grams are laid out one n × n block per split, so only a
+// single-patch scale (the global patch) is split.
 int choose_split(int64_t np, int n, int L) {
+  if (np != 1) return 1;
   const int T = (n + kTile - 1) / kTile;
   const int64_t ctas = (int64_t)T * (T + 1) / 2 * np;
   if (ctas >= 592) return 1;
@@ -766,6 +769,137 @@ int patch_nucnorm_all(Ctx* c, const cf* X, double* reg_out, cudaStream_t st) {
     reg += c->lambdas[k] * sk;
   }
   *reg_out = reg;
+  return MSLR_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// Patch-SVST backward (used by the unrolled-POGM gradient, grad.cu)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct VjpPtrs {
+  cf* gram;     // np × n × n: G, then the Householder vectors
+  cf* V;        // np × n × n: eigenvectors (row-major)
+  double* aux;  // np × n × n: FP64 scratch of the eigen stage
+  int* rank;    // np
+  double* lam;  // np × n eigenvalues (descending)
+  cf* wbar;     // W̄, then W
+  cf* t1;       // W̄ V, then V diag(f), then V E
+  cf* d;        // Vᴴ W̄ V, then K
+  cf* e;        // F ⊙ (D + Dᴴ)
+  double* bbar; // np
+  cf* part;     // split-K partial products of the single-patch scale
+};
+
+int xsplit_of(int64_t np, int n, int L) {
+  if (np != 1) return 1;
+  const int T = (n + kTile - 1) / kTile;
+  return std::max(1, std::min((592 + T * T - 1) / (T * T), std::max(1, L / 1024)));
+}
+
+size_t vjp_bytes(int64_t np, int n, int nsplit) {
+  const size_t nn = (size_t)n * n;
+  return np * nn * sizeof(cf) * 6 + np * nn * sizeof(double) + np * sizeof(int) +
+         np * (size_t)n * sizeof(double) + np * sizeof(double) + (size_t)nsplit * nn * sizeof(cf) +
+         11 * 256;
+}
+
+VjpPtrs carve_vjp(void* base, int64_t np, int n, int nsplit) {
+  const size_t nn = (size_t)n * n;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  unsigned char* p = reinterpret_cast<unsigned char*>(base);
+  auto take = [&](size_t bytes) {
+    unsigned char* q = p;
+    p += al(bytes);
+    return q;
+  };
+  VjpPtrs v;
+  v.gram = reinterpret_cast<cf*>(take(np * nn * sizeof(cf)));
+  v.V = reinterpret_cast<cf*>(take(np * nn * sizeof(cf)));
+  v.aux = reinterpret_cast<double*>(take(np * nn * sizeof(double)));
+  v.rank = reinterpret_cast<int*>(take(np * sizeof(int)));
+  v.lam = reinterpret_cast<double*>(take(np * (size_t)n * sizeof(double)));
+  v.wbar = reinterpret_cast<cf*>(take(np * nn * sizeof(cf)));
+  v.t1 = reinterpret_cast<cf*>(take(np * nn * sizeof(cf)));
+  v.d = reinterpret_cast<cf*>(take(np * nn * sizeof(cf)));
+  v.e = reinterpret_cast<cf*>(take(np * nn * sizeof(cf)));
+  v.bbar = reinterpret_cast<double*>(take(np * sizeof(double)));
+  v.part = reinterpret_cast<cf*>(take((size_t)nsplit * nn * sizeof(cf)));
+  return v;
+}
+
+int nsplit_vjp(const ScaleGeom& g) {
+  return std::max(choose_split(g.Np, g.n, g.L), xsplit_of(g.Np, g.n, g.L));
+}
+
+}  // namespace
+
+int svst_vjp_setup(Ctx* c) {
+  size_t need = 0;
+  for (auto& g : c->scales) need = std::max(need, vjp_bytes(g.Np, g.n, nsplit_vjp(g)));
+  if (need <= c->vjpw_bytes) return MSLR_OK;
+  if (c->d_vjpw) cudaFree(c->d_vjpw);
+  c->d_vjpw = nullptr;
+  c->vjpw_bytes = 0;
+  int rc;
+  if ((rc = dalloc(c, &c->d_vjpw, need))) return rc;
+  c->vjpw_bytes = need;
+  return MSLR_OK;
+}
+
+// zbar = J_prox(z)ᴴ xbar for scale s (patch SVST with threshold β), and
+// *bbar = ∂⟨xbar, prox(z)⟩/∂β.  tmp: one image of scratch.
+int svst_vjp_scale(Ctx* c, int s, const cf* z, const cf* xbar, double beta, cf* zbar, cf* tmp,
+                   double* bbar, cudaStream_t st) {
+  const ScaleGeom& g = c->scales[s];
+  const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
+  const int64_t np = g.Np;
+  const int n = g.n;
+  const VjpPtrs v = carve_vjp(c->d_vjpw, np, n, nsplit_vjp(g));
+  int rc;
+  const cf* ob = xbar;
+  if (!g.partition) {
+    if ((rc = div_count_launch(xbar, m, g.d_cover, tmp, st))) return rc;
+    ob = tmp;
+  }
+  WorkPtrs w{};
+  w.gram = v.gram;
+  w.zv = v.V;
+  w.aux = v.aux;
+  w.rank = v.rank;
+  w.part = v.part;
+  if ((rc = svst_gram(z, m, np, w, choose_split(np, n, g.L), false, st, &c->launches))) return rc;
+  EigSegment seg;
+  seg.n = n;
+  seg.np = np;
+  seg.gram = v.gram;
+  seg.zv = v.V;
+  seg.aux = v.aux;
+  seg.rank = v.rank;
+  seg.lam = 0.0;
+  seg.lam_out = v.lam;
+  if ((rc = eig_launch_multi(1, &seg, c->d_thr, 0, st))) return rc;
+  if ((rc = xgram_launch(ob, z, m, np, v.wbar, v.part, xsplit_of(np, n, g.L), st))) return rc;
+  if ((rc = bgemm_launch(0, 0, v.wbar, v.V, v.t1, n, np, st))) return rc;         // W̄ V
+  if ((rc = bgemm_launch(1, 0, v.V, v.t1, v.d, n, np, st))) return rc;            // D = Vᴴ W̄ V
+  if ((rc = divdiff_launch(v.d, v.lam, v.V, beta, n, np, v.e, v.t1, v.bbar, st))) return rc;
+  if ((rc = bgemm_launch(0, 1, v.t1, v.V, v.wbar, n, np, st))) return rc;         // W = V f Vᴴ
+  if ((rc = bgemm_launch(0, 0, v.V, v.e, v.t1, n, np, st))) return rc;            // V E
+  if ((rc = bgemm_launch(0, 1, v.t1, v.V, v.d, n, np, st))) return rc;            // K = V E Vᴴ
+  if (g.partition) {
+    if ((rc = vjp_rebuild_launch(ob, z, v.wbar, v.d, m, np, zbar, 1, st))) return rc;
+  } else {
+    if ((rc = vjp_rebuild_launch(ob, z, v.wbar, v.d, m, np, c->d_pbuf, 0, st))) return rc;
+    if ((rc = patch_sum_launch(c->d_pbuf, m, g.d_cover, zbar, st))) return rc;
+  }
+  c->launches += 11;
+  std::vector<double> hb((size_t)np);
+  MSLR_CUDA_TRY(cudaMemcpyAsync(hb.data(), v.bbar, np * sizeof(double), cudaMemcpyDeviceToHost, st));
+  MSLR_CUDA_TRY(cudaStreamSynchronize(st));
+  double t = 0.0;
+  for (double x : hb) t += x;
+  *bbar = t;
   return MSLR_OK;
 }
 

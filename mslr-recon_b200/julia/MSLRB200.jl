@@ -20,7 +20,7 @@ module MSLRB200
 using CUDA
 
 export MSLRContext, sense_forward!, sense_adjoint!, dc_cost_grad!, patch_svst!,
-       pogm_run!, power_iter, mslr_lambdas
+       pogm_run!, power_iter, mslr_lambdas, set_lambdas!, pogm_grad
 
 const libmslr = get(ENV, "MSLR_LIB", joinpath(@__DIR__, "..", "libmslr.so"))
 
@@ -178,6 +178,43 @@ function power_iter(ctx::MSLRContext; niter::Integer=200, tol::Real=1e-6)
                  (Ptr{Cvoid}, Int32, Float64, Ref{Float64}, Ref{Int32}, Ptr{Cvoid}),
                  ctx.h, Int32(niter), Float64(tol), s1, it, _stream()), ctx.h)
     return s1[], Int(it[])
+end
+
+"""
+    set_lambdas!(ctx, λs)
+
+Per-scale weights λ_k of g_prox (`c * λs[k]`, scripts/reconstruct.jl:196-202);
+the context starts from the Ong–Lustig values of :164-169.
+"""
+function set_lambdas!(ctx::MSLRContext, λs::AbstractVector{<:Real})
+    length(λs) == ctx.Ns || throw(ArgumentError("need $(ctx.Ns) lambdas"))
+    _check(ccall((:mslr_set_lambdas, libmslr), Cint, (Ptr{Cvoid}, Ptr{Float64}),
+                 ctx.h, Float64.(collect(λs))), ctx.h)
+    return ctx
+end
+
+"""
+    pogm_grad(ctx, X_true, niter, L; restart_cutoff=0.0, bsig=1.0) -> (loss, ∂loss/∂log λ, X, restarts)
+
+Runs `pogm_run!`'s iteration for `niter` steps from X0 = A'y and returns
+loss = ½‖Σ_k X[..,k] − X_true‖² (X_true `(Nx,Ny,Nz,Nt)`), its gradient with
+respect to log λ_k (reverse accumulation through the SENSE normal operator
+and the patch-SVST backward, restart decisions held fixed), the final X and
+the restart flags.
+"""
+function pogm_grad(ctx::MSLRContext, X_true::CuArray{ComplexF32}, niter::Integer, L::Real;
+                   restart_cutoff::Real=0.0, bsig::Real=1.0)
+    size(X_true) == (ctx.N..., ctx.Nt) || throw(ArgumentError("X_true size $(size(X_true))"))
+    X = CuArray{ComplexF32}(undef, ctx.N..., ctx.Nt, ctx.Ns)
+    loss = Ref{Float64}(0.0)
+    grad = zeros(Float64, ctx.Ns)
+    flags = zeros(UInt8, niter + 1)
+    _check(ccall((:mslr_pogm_grad, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, Int32, Float64, Float64, Float64, CuPtr{ComplexF32},
+                  Ref{Float64}, Ptr{Float64}, Ptr{UInt8}, Ptr{Cvoid}),
+                 ctx.h, X_true, Int32(niter), Float64(L), Float64(restart_cutoff), Float64(bsig), X,
+                 loss, grad, flags, _stream()), ctx.h)
+    return loss[], grad, X, Bool.(flags)
 end
 
 """Ong–Lustig λ_k of scripts/reconstruct.jl:164-169."""

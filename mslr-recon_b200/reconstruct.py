@@ -74,3 +74,43 @@ def run_recon(smaps, y, idx, patch_sizes, strides, niters: int, sigma1=None, for
         if return_components:
             out["X"] = X.cpu().numpy()
     return out
+
+
+def run_recon_kspace(ksp, smaps_raw, patch_sizes, strides, niters: int, sigma1=None, form: str = "tuned",
+                     power_niter: int = 200, power_tol: float = 1e-6, restart_cutoff: float = 0.0,
+                     bsig: float = 1.0):
+    """run_recon from its raw inputs (scripts/reconstruct.jl:86-226): the
+    zero-filled k-space ksp (Nt, Nc, Nz, Ny, Nx) and raw coil maps
+    (Nc, Nz, Ny, Nx).  Maps normalisation, the 99th-percentile scaling, the
+    sampling mask and its checks and the sample gathering run on the device
+    (``MSLRContext.prepare``); then σ₁, X0 and POGM as :func:`run_recon`.
+    Returns its dict plus ``scale_factor``, ``omega_counts`` (K) and the
+    device-prepared ``smaps``, ``y`` and ``idx`` on the host."""
+    from .context import sampling
+    dev = torch.device("cuda")
+    ksp_t = torch.as_tensor(ksp).to(dev, torch.complex64).contiguous()
+    sm_t = torch.as_tensor(smaps_raw).to(dev, torch.complex64).contiguous()
+    Nt, Nc, Nz, Ny, Nx = ksp_t.shape
+    K = sampling(ksp_t)
+    with MSLRContext((Nx, Ny, Nz), Nc, Nt, K, patch_sizes, strides, form=form) as ctx:
+        smaps, y, idx, scale = ctx.prepare(ksp_t, sm_t)
+        if sigma1 is None:
+            sigma1, _ = ctx.power_iter(power_niter, power_tol)
+        L = ctx.Ns * float(sigma1) ** 2
+        X = ctx.init_x0()
+        restarts = ctx.pogm_run(X, niters, L, restart_cutoff, bsig)
+        torch.cuda.synchronize()
+        return {
+            "X_recon": X.sum(dim=0).cpu().numpy(),
+            "X": X.cpu().numpy(),
+            "restarts": restarts,
+            "lambdas": list(ctx.lambdas),
+            "sigma1A": float(sigma1),
+            "L": L,
+            "scale_factor": scale,
+            "omega_counts": K,
+            "smaps": smaps.cpu().numpy(),
+            "y": y.cpu().numpy(),
+            "idx": idx.cpu().numpy(),
+            "Niters": niters,
+        }

@@ -636,3 +636,78 @@ def pogm_unrolled_grad(prob: ReconProblem, niter: int, X_true: np.ndarray, lambd
         xbar = wv - alpha * hw[None] - gamma * zbar
         ubar = -beta * zbar
     return loss, grad, X, restarts
+
+
+# ---------------------------------------------------------------------------
+# Setup of run_recon — scripts/reconstruct.jl:86-147, src/recon.jl:310-321
+# ---------------------------------------------------------------------------
+class SetupError(ValueError):
+    """The reference's @assert failures of scripts/reconstruct.jl:113-118."""
+
+
+def sos_normalize_maps(smaps_raw: np.ndarray) -> np.ndarray:
+    """scripts/reconstruct.jl:89: ``S ./ (sqrt.(sum(abs2.(S); dims=4)) .+ eps(Float32))``
+    in Float32, coils summed in order.  smaps_raw (Nc, Nz, Ny, Nx) complex64."""
+    S = smaps_raw.astype(np.complex64)
+    acc = np.zeros(S.shape[1:], dtype=np.float32)
+    for c in range(S.shape[0]):
+        acc = acc + (S[c].real * S[c].real + S[c].imag * S[c].imag)
+    den = np.sqrt(acc) + np.finfo(np.float32).eps
+    out = np.empty_like(S)
+    out.real = S.real / den
+    out.imag = S.imag / den
+    return out
+
+
+def sense_comb(ksp: np.ndarray, smaps: np.ndarray) -> np.ndarray:
+    """src/recon.jl:310-321 on the zero-filled k-space ksp (Nt, Nc, Nz, Ny, Nx):
+    Σ_c conj(S_c)·fftshift(ifft(ifftshift(ksp_c))) / (Σ_c |S_c|² + eps()),
+    the denominator and the division in Float64, the image stored as
+    ComplexF32."""
+    den = np.sum(np.abs(smaps.astype(np.complex128)) ** 2, axis=0) + np.finfo(np.float64).eps
+    img = np.empty((ksp.shape[0],) + ksp.shape[2:], dtype=np.complex64)
+    for t in range(ksp.shape[0]):
+        mc = sfft.fftshift(sfft.ifftn(sfft.ifftshift(ksp[t].astype(np.complex128), axes=SPATIAL_AXES),
+                                      axes=SPATIAL_AXES), axes=SPATIAL_AXES)
+        num = np.sum(np.conj(smaps.astype(np.complex128)) * mc, axis=0)
+        img[t] = (num / den).astype(np.complex64)
+    return img
+
+
+def quantile_type7(v: np.ndarray, p: float) -> float:
+    """Statistics.quantile (Hyndman–Fan type 7) as Julia evaluates it for a
+    Float32 vector: a + γ·(b − a) with (b − a) in Float32 and the rest in
+    Float64."""
+    v = np.sort(np.asarray(v, dtype=np.float32).ravel())
+    n = v.size
+    h = (n - 1) * p
+    j = int(math.floor(h))
+    g = h - j
+    a = v[j]
+    b = v[min(j + 1, n - 1)]
+    return float(a) + g * float(np.float32(b - a))
+
+
+def prepare_kspace(ksp: np.ndarray, smaps_raw: np.ndarray):
+    """scripts/reconstruct.jl:86-147 from the zero-filled k-space ksp
+    (Nt, Nc, Nz, Ny, Nx) and raw coil maps (Nc, Nz, Ny, Nx).  Returns
+    (smaps, y (Nt, Nc, K), idx (Nt, K) 0-based, scale_factor)."""
+    smaps = sos_normalize_maps(smaps_raw)
+    img0 = sense_comb(ksp, smaps)
+    mags = np.abs(img0.astype(np.complex128)).astype(np.float32)
+    scale = quantile_type7(mags, 0.99)
+    div = max(scale, float(np.finfo(np.float32).eps))
+    k = (ksp.astype(np.complex128) / div).astype(np.complex64)
+    Nt, Nc = k.shape[:2]
+    flat = k.reshape(Nt, Nc, -1)
+    omega = flat[:, 0] != 0
+    for c in range(1, Nc):
+        if not np.array_equal(omega, flat[:, c] != 0):
+            raise SetupError(f"Coil {c + 1} has a different sampling pattern")
+    counts = omega.sum(axis=1)
+    for t in range(1, Nt):
+        if counts[t] != counts[t - 1]:
+            raise SetupError(f"Frame {t + 1} has a different sample count")
+    idx = np.stack([np.flatnonzero(omega[t]) for t in range(Nt)]).astype(np.int32)
+    y = np.stack([flat[t][:, idx[t]] for t in range(Nt)])
+    return smaps, y, idx, scale
