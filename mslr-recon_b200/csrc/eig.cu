@@ -31,7 +31,9 @@
 //      columns beyond the rank set to zero.
 // Zero patches give no eigenvalue above β² and Ṽ = 0, hence W = 0 (the
 // reference's zero-norm skip, src/recon.jl:185).
+#include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "internal.h"
 
@@ -746,29 +748,32 @@ int eig2_prepare(int nmax) {
   return MSLR_OK;
 }
 
-int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int thr_per_patch,
+namespace {
+
+// One launch over segments that all take the same CTA variant.
+int eig_launch_group(const std::vector<const EigSegment*>& segs, const double* thr, int thr_per_patch,
                      cudaStream_t st) {
-  if (nseg < 1 || nseg > kMaxSeg) return fail(MSLR_ERR_UNSUPPORTED, "too many scales in one launch");
   EigArgs a;
-  a.nseg = nseg;
+  a.nseg = (int)segs.size();
   a.thr = thr;
   a.thr_per_patch = thr_per_patch;
   int64_t total = 0;
   int nmax = 1;
-  for (int s = 0; s < nseg; ++s) {
+  for (int s = 0; s < a.nseg; ++s) {
     Seg& S = a.seg[s];
-    S.n = segs[s].n;
+    const EigSegment& e = *segs[s];
+    S.n = e.n;
     S.first = total;
-    S.np = segs[s].np;
-    S.gram = segs[s].gram;
-    S.zv = segs[s].zv;
-    S.aux = segs[s].aux;
-    S.rank = segs[s].rank;
-    S.lam = segs[s].lam;
-    S.nuc = segs[s].nuc;
-    S.lam_out = segs[s].lam_out;
-    total += segs[s].np;
-    nmax = std::max(nmax, segs[s].n);
+    S.np = e.np;
+    S.gram = e.gram;
+    S.zv = e.zv;
+    S.aux = e.aux;
+    S.rank = e.rank;
+    S.lam = e.lam;
+    S.nuc = e.nuc;
+    S.lam_out = e.lam_out;
+    total += e.np;
+    nmax = std::max(nmax, e.n);
   }
   const int threads = nmax <= kSmallT ? kSmallT : kT;
   a.rz = stage_cols(nmax, threads);
@@ -779,6 +784,26 @@ int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int th
     k_eig<kT, 1><<<(unsigned)total, kT, sm, st>>>(a);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
+}
+
+}  // namespace
+
+// Segments with Gram side <= 384 run in the 384-thread variant (two patches per
+// SM), larger ones in the 1024-thread variant: one launch per variant present.
+// Per-patch thresholds (thr_per_patch) index patches across all segments, so
+// such calls keep every segment in one launch.
+int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int thr_per_patch,
+                     cudaStream_t st) {
+  if (nseg < 1 || nseg > kMaxSeg) return fail(MSLR_ERR_UNSUPPORTED, "too many scales in one launch");
+  std::vector<const EigSegment*> small, big, all;
+  for (int s = 0; s < nseg; ++s) {
+    (segs[s].n <= kSmallT ? small : big).push_back(&segs[s]);
+    all.push_back(&segs[s]);
+  }
+  if (thr_per_patch || small.empty() || big.empty()) return eig_launch_group(all, thr, thr_per_patch, st);
+  int rc = eig_launch_group(big, thr, 0, st);
+  if (!rc) rc = eig_launch_group(small, thr, 0, st);
+  return rc;
 }
 
 int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, const double* thr,

@@ -579,7 +579,11 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     segs[k].lam = c->lambdas[k];
   }
   if ((rc = eig_launch_multi(c->Ns, segs.data(), thr_dev, 0, st))) return rc;
-  c->launches += 1;
+  {
+    bool small = false, big = false;   // one eigen launch per CTA variant present
+    for (const auto& sg : segs) (sg.n <= 384 ? small : big) = true;
+    c->launches += (small && big) ? 2 : 1;
+  }
   for (int k = 0; k < c->Ns; ++k)
     if ((rc = svst_form_w(ws[k], c->scales[k].n, c->scales[k].Np, true, st, &c->launches))) return rc;
   for (int k = 0; k < c->Ns; ++k) {

@@ -324,3 +324,34 @@ def test_normal_op_tensor_core_plane_pass(torch, M, monkeypatch):
     (split-BF16 products), and the POGM-facing forward / adjoint unchanged."""
     monkeypatch.setenv("MSLR_XY_PATH", "tc")
     test_sense_metric_shapes(torch, M, "tuned-tc", (90, 90, 60), 18)
+
+
+def test_mixed_gram_sides_per_iteration(torch, M):
+    """Scales whose Gram sides need both eigen variants (400 > 384 and 64) in
+    one tuned-form iteration: X after every iteration within 1e-4 of the FP64
+    oracle, identical restart flags."""
+    rng = np.random.default_rng(31)
+    N, Nc, Nt = (16, 16, 8), 2, 400
+    nvox = N[0] * N[1] * N[2]
+    K = nvox // 3
+    smaps = rng.standard_normal((Nc, N[2], N[1], N[0])) + 1j * rng.standard_normal((Nc, N[2], N[1], N[0]))
+    smaps /= np.sqrt((np.abs(smaps) ** 2).sum(0))[None]
+    idx = np.stack([np.sort(rng.choice(nvox, K, replace=False)) for _ in range(Nt)]).astype(np.int32)
+    U = rng.standard_normal((nvox, 3)) + 1j * rng.standard_normal((nvox, 3))
+    V = rng.standard_normal((Nt, 3)) + 1j * rng.standard_normal((Nt, 3))
+    x = (V @ U.T).reshape(Nt, N[2], N[1], N[0]) * 10
+    y = O.sense_forward(x, smaps, idx) + 0.05 * (rng.standard_normal((Nt, Nc, K)) + 1j * rng.standard_normal((Nt, Nc, K)))
+    ps = [[16, 16, 8], [4, 4, 4]]
+    prob = O.ReconProblem(smaps=smaps, idx=idx, y=y, patch_sizes=ps, strides=ps, sigma1=1.0)
+    traj = []
+    _, restarts, _, _ = O.run_recon_arrays(prob, 3, iter_callback=lambda it, xk, r: traj.append(xk.copy()))
+    with M.MSLRContext(N, Nc, Nt, K, ps, ps, form="tuned") as ctx:
+        ctx.bind(dev(torch, smaps), dev(torch, y), dev(torch, idx, torch.int32))
+        X = ctx.init_x0()
+        ctx.pogm_begin(X, 3, L=2.0)
+        errs = []
+        for i in range(3):
+            ctx.pogm_step(X)
+            errs.append(rel(X.cpu().numpy(), traj[i]))
+        assert max(errs) < 1e-4, errs
+        assert ctx.pogm_restarts() == restarts
