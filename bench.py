@@ -82,7 +82,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--form", default="tuned", choices=["tuned", "plain"])
+    p.add_argument("--form", default="tuned", choices=["tuned", "plain", "tf32"])
     p.add_argument("--workload", default=WORKLOAD)
     p.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")

@@ -52,6 +52,7 @@ extern "C" {
 /* Computation forms (mslr_create `form`). */
 #define MSLR_FORM_PLAIN 0        /* FP32 SIMT Gram/rebuild, one launch sequence per scale, no graph */
 #define MSLR_FORM_TUNED 1        /* split-precision tensor-core Gram/rebuild, graph-captured iteration */
+#define MSLR_FORM_TF32 2         /* as TUNED with TF32 (not split) tensor-core Gram/rebuild products */
 
 typedef struct mslr_ctx mslr_ctx;
 

@@ -22,6 +22,7 @@ MSLR_ERR_NOMEM = 6
 
 FORM_PLAIN = 0
 FORM_TUNED = 1
+FORM_TF32 = 2
 
 # name -> (restype, argtypes)
 _P = C.c_void_p

@@ -15,9 +15,9 @@ import math
 import numpy as np
 import torch
 
-from ._lib import FORM_PLAIN, FORM_TUNED, check, i32arr, lib
+from ._lib import FORM_PLAIN, FORM_TF32, FORM_TUNED, check, i32arr, lib
 
-FORMS = {"plain": FORM_PLAIN, "tuned": FORM_TUNED}
+FORMS = {"plain": FORM_PLAIN, "tuned": FORM_TUNED, "tf32": FORM_TF32}
 
 
 def _stream_ptr(stream=None) -> int:

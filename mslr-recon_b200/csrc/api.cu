@@ -151,7 +151,8 @@ int mslr_svst_batch(int32_t m, int32_t n, int32_t batch, const double* betas, co
   for (int b = 0; b < batch; ++b)
     if (!(betas[b] >= 0.0) || !std::isfinite(betas[b]))
       return fail(MSLR_ERR_ARG, "thresholds must be finite and non-negative");
-  if (form != MSLR_FORM_PLAIN && form != MSLR_FORM_TUNED) return fail(MSLR_ERR_ARG, "unknown form");
+  if (form != MSLR_FORM_PLAIN && form != MSLR_FORM_TUNED && form != MSLR_FORM_TF32)
+    return fail(MSLR_ERR_ARG, "unknown form");
   return svst_batch(m, n, batch, betas, reinterpret_cast<const cf*>(in), reinterpret_cast<cf*>(out),
                     workspace, workspace_bytes, form, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -175,7 +176,8 @@ int mslr_create(const int32_t N[3], int32_t Nc, int32_t Nt, int64_t K, int32_t n
   if (!N || !patch || !stride) return fail(MSLR_ERR_ARG, "null argument");
   if (N[0] <= 0 || N[1] <= 0 || N[2] <= 0 || Nc <= 0 || Nt <= 0 || K <= 0 || n_scales <= 0)
     return fail(MSLR_ERR_ARG, "dimensions, coils, frames, samples and scales must be positive");
-  if (form != MSLR_FORM_PLAIN && form != MSLR_FORM_TUNED) return fail(MSLR_ERR_ARG, "unknown form");
+  if (form != MSLR_FORM_PLAIN && form != MSLR_FORM_TUNED && form != MSLR_FORM_TF32)
+    return fail(MSLR_ERR_ARG, "unknown form");
   const int64_t nvox = (int64_t)N[0] * N[1] * N[2];
   if (K > nvox) return fail(MSLR_ERR_ARG, "more samples per frame than k-space points");
   mslr_ctx* c = new mslr_ctx();

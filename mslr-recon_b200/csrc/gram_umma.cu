@@ -15,6 +15,11 @@
 //   rebuild  Re += Ar·Brᵀ − Ai·Biᵀ      Im += Ar·Biᵀ + Ai·Brᵀ
 // (negation through the instruction descriptor).
 //
+// The TF32 form runs the same products with TF32 operands (one FP32 plane per
+// part, rounded to TF32) and four M=128 × N=128 × K=8 kind::tf32 MMAs per
+// 8-element K step: Gram Re += Ar·Brᵀ + Ai·Biᵀ, Im += Ai·Brᵀ − Ar·Biᵀ (the
+// rebuild's signs as above).
+//
 // One CTA of 8 warps per 128 × 128 output tile.  K advances 32 elements per
 // chunk: every thread loads its share of the next chunk from global memory
 // into registers (patch element addresses from per-row / per-K offset
@@ -141,6 +146,38 @@ __device__ __forceinline__ void split_pair(float x0, float x1, uint32_t& hi, uin
   lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
+// TF32 operands (the TF32 form): one FP32 plane per real / imaginary part,
+// each value rounded to TF32 (to nearest, ties away), in K-major unswizzled
+// core matrices of 8 rows × 4 values (128 bytes): k-adjacent cores 128 B apart
+// (LBO), 8-row groups 1024 B apart (SBO).  A chunk of 32 K values is four
+// 8-value MMA steps.  Planes per stage: Ar, Ai, Br, Bi of 4096 words each.
+constexpr int kTfPlane = kTile;   // words per TF32 plane (128 rows × 32 values)
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ int tf_word(int r, int k) {
+  return ((r >> 3) * 8 + (k >> 2)) * 32 + (r & 7) * 4 + (k & 3);
+}
+__device__ __forceinline__ uint64_t sdesc_tf(const void* p) {
+  const uint64_t a = su32(p);
+  return ((a >> 4) & 0x3FFFull) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         (1ull << 46);
+}
+// instruction descriptor: TF32 × TF32 → F32, both K-major, M = 128, N = 128
+__host__ __device__ constexpr uint32_t idesc_tf(bool negA) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((negA ? 1u : 0u) << 13) | ((uint32_t)(kTN >> 3) << 17) |
+         ((uint32_t)(kTM >> 4) << 24);
+}
+__device__ __forceinline__ void umma_tf(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t id, bool acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+      "l"(a), "l"(b), "r"(id), "r"(acc ? 1u : 0u));
+}
+
 // Registers of one operand chunk: thread t holds pairs q = t + 256 i, i < 8, of
 // the 128 × 32 tile; pair q is (row r, k..k+1) of core c = q / 32.
 struct Chunk {
@@ -189,6 +226,28 @@ __device__ __forceinline__ void store_chunk(const Chunk& ch, uint32_t* rh, uint3
   }
 }
 
+// One operand chunk into stage `stage` (B operand when isB), conjugated when conj.
+template <bool TF>
+__device__ __forceinline__ void store_operand(const Chunk& ch, uint32_t* stage, bool isB, bool conj) {
+  if constexpr (TF) {
+    uint32_t* re = stage + (isB ? 2 : 0) * kTfPlane;
+    uint32_t* im = stage + (isB ? 3 : 1) * kTfPlane;
+#pragma unroll
+    for (int i = 0; i < kPairs; ++i) {
+      int r, k;
+      pair_rk(i, r, k);
+      const int w = tf_word(r, k);
+      const cf a = ch.v[i][0], b = ch.v[i][1];
+      *reinterpret_cast<uint2*>(re + w) = make_uint2(to_tf32(a.x), to_tf32(b.x));
+      *reinterpret_cast<uint2*>(im + w) = make_uint2(to_tf32(conj ? -a.y : a.y), to_tf32(conj ? -b.y : b.y));
+    }
+  } else {
+    const int o = isB ? BR_H : AR_H;
+    store_chunk(ch, stage + (o + 0) * (kTile / 2), stage + (o + 1) * (kTile / 2),
+                stage + (o + 2) * (kTile / 2), stage + (o + 3) * (kTile / 2), conj);
+  }
+}
+
 // The 12 MMAs of one 16-element K step t of stage s.
 template <bool GRAM>
 __device__ __forceinline__ void issue_step(const USmem& s, int st, int t, uint32_t dre, uint32_t dim,
@@ -223,9 +282,39 @@ __device__ __forceinline__ void issue_step(const USmem& s, int st, int t, uint32
   }
 }
 
+// All MMAs of the chunk in stage st (first: the accumulators start from zero).
+template <bool GRAM, bool TF>
+__device__ __forceinline__ void issue_chunk(const USmem& s, int st, uint32_t dre, uint32_t dim,
+                                            bool first, bool bSameAsA) {
+  if constexpr (TF) {
+    const uint32_t* o = &s.op[st][0][0];
+    const int br = bSameAsA ? 0 : 2, bi = bSameAsA ? 1 : 3;
+    constexpr uint32_t P = idesc_tf(false), N = idesc_tf(true);
+#pragma unroll
+    for (int t = 0; t < kKc / 8; ++t) {
+      auto D = [&](int pl) { return sdesc_tf(o + pl * kTfPlane + t * 64); };   // +2 cores = 256 B
+      const bool acc = !first || t > 0;
+      // Gram:    Re += Ar·Brᵀ + Ai·Biᵀ   Im += Ai·Brᵀ − Ar·Biᵀ
+      // rebuild: Re += Ar·Brᵀ − Ai·Biᵀ   Im += Ar·Biᵀ + Ai·Brᵀ
+      umma_tf(dre, D(0), D(br), P, acc);
+      umma_tf(dre, D(1), D(bi), GRAM ? P : N, true);
+      if (GRAM) {
+        umma_tf(dim, D(1), D(br), P, acc);
+        umma_tf(dim, D(0), D(bi), N, true);
+      } else {
+        umma_tf(dim, D(0), D(bi), P, acc);
+        umma_tf(dim, D(1), D(br), P, true);
+      }
+    }
+  } else {
+    issue_step<GRAM>(s, st, 0, dre, dim, !first, bSameAsA);
+    issue_step<GRAM>(s, st, 1, dre, dim, true, bSameAsA);
+  }
+}
+
 // Main loop shared by both kernels: nch chunks; kofs(c, buf) fills s.kof[buf]
 // for chunk c (threads < 32); returns false on a timed-out wait.
-template <bool GRAM, class KOfs>
+template <bool GRAM, bool TF, class KOfs>
 __device__ __forceinline__ bool mainloop(USmem& s, int nch, const cf* abase, const cf* bbase,
                                          bool conjA, bool conjB, bool bSameAsA, const KOfs& kofs) {
   const int tid = threadIdx.x;
@@ -240,9 +329,8 @@ __device__ __forceinline__ bool mainloop(USmem& s, int nch, const cf* abase, con
     if (c + 1 < nch) kofs(c + 1, (c + 1) & 1);
     if (c >= 2 && ok && !mbar_wait(&s.bar[st], (unsigned)(((c - 2) >> 1) & 1))) ok = false;
     if (ok) {
-      store_chunk(ca, s.op[st][AR_H], s.op[st][AR_L], s.op[st][AI_H], s.op[st][AI_L], conjA);
-      if (!bSameAsA)
-        store_chunk(cb, s.op[st][BR_H], s.op[st][BR_L], s.op[st][BI_H], s.op[st][BI_L], conjB);
+      store_operand<TF>(ca, &s.op[st][0][0], false, conjA);
+      if (!bSameAsA) store_operand<TF>(cb, &s.op[st][0][0], true, conjB);
     }
     fence_async_smem();
     __syncthreads();
@@ -252,8 +340,7 @@ __device__ __forceinline__ bool mainloop(USmem& s, int nch, const cf* abase, con
     }
     if (tid == 0 && ok) {
       tc_fence_after();
-      issue_step<GRAM>(s, st, 0, s.tmem, s.tmem + kTN, c > 0, bSameAsA);
-      issue_step<GRAM>(s, st, 1, s.tmem, s.tmem + kTN, true, bSameAsA);
+      issue_chunk<GRAM, TF>(s, st, s.tmem, s.tmem + kTN, c == 0, bSameAsA);
       umma_commit(&s.bar[st]);
     }
     ok = __syncthreads_and(ok);
@@ -288,6 +375,7 @@ __device__ __forceinline__ void tmem_free(USmem& s) {
 }
 
 // ---------------------------------------------------------------------------
+template <bool TF>
 __global__ void __launch_bounds__(kThr, 1)
     k_gram_umma(const cf* __restrict__ img, PatchMap m, cf* __restrict__ out, int nsplit,
                 int lchunk, int* __restrict__ err) {
@@ -326,7 +414,7 @@ __global__ void __launch_bounds__(kThr, 1)
   tc_fence_after();
   const cf* base = img + org;
   const bool cj = m.tall != 0;
-  const bool ok = mainloop<true>(s, nch, base, base, cj, cj, diag, kofs);
+  const bool ok = mainloop<true, TF>(s, nch, base, base, cj, cj, diag, kofs);
   cf* G = out + ((nsplit > 1) ? (int64_t)split * n * n : ip * (int64_t)n * n);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int a = a0 + (warp & 3) * 32 + lane;
@@ -361,6 +449,7 @@ __global__ void __launch_bounds__(kThr, 1)
 }
 
 // ---------------------------------------------------------------------------
+template <bool TF>
 __global__ void __launch_bounds__(kThr, 1)
     k_rebuild_umma(const cf* __restrict__ img, const cf* __restrict__ W, PatchMap m,
                    cf* __restrict__ out, int direct, int* __restrict__ err) {
@@ -421,9 +510,8 @@ __global__ void __launch_bounds__(kThr, 1)
       if (c + 1 < nch) kofs(c + 1, (c + 1) & 1);
       if (c >= 2 && good && !mbar_wait(&s.bar[st], (unsigned)(((c - 2) >> 1) & 1))) good = false;
       if (good) {
-        store_chunk(ca, s.op[st][AR_H], s.op[st][AR_L], s.op[st][AI_H], s.op[st][AI_L], true);
-        store_chunk(cb, s.op[st][BR_H], s.op[st][BR_L], s.op[st][BI_H], s.op[st][BI_L],
-                    m.tall != 0);
+        store_operand<TF>(ca, &s.op[st][0][0], false, true);
+        store_operand<TF>(cb, &s.op[st][0][0], true, m.tall != 0);
       }
       fence_async_smem();
       __syncthreads();
@@ -433,8 +521,7 @@ __global__ void __launch_bounds__(kThr, 1)
       }
       if (threadIdx.x == 0 && good) {
         tc_fence_after();
-        issue_step<false>(s, st, 0, s.tmem, s.tmem + kTN, c > 0, false);
-        issue_step<false>(s, st, 1, s.tmem, s.tmem + kTN, true, false);
+        issue_chunk<false, TF>(s, st, s.tmem, s.tmem + kTN, c == 0, false);
         umma_commit(&s.bar[st]);
       }
       good = __syncthreads_and(good);
@@ -518,32 +605,42 @@ int umma_prepare() {
   MSLR_CUDA_TRY(cudaGetDevice(&dev));
   std::lock_guard<std::mutex> lk(mu);
   if (dev < 64 && done[dev]) return MSLR_OK;
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_gram_umma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_gram_umma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(USmem)));
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_rebuild_umma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_rebuild_umma<false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(USmem)));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_gram_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(USmem)));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_rebuild_umma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(USmem)));
   if (dev < 64) done[dev] = true;
   return MSLR_OK;
 }
 
 int gram_umma_launch(const cf* img, const PatchMap& m, int64_t np, cf* out_or_part, int nsplit,
-                     int lchunk, cudaStream_t st) {
+                     int lchunk, cudaStream_t st, bool tf32) {
   if (int rc = umma_prepare()) return rc;
   int* err = umma_err_ptr();
   const int T = (m.n + kTM - 1) / kTM;
   const int ntri = T * (T + 1) / 2;
-  k_gram_umma<<<dim3(ntri, (unsigned)np, nsplit), kThr, sizeof(USmem), st>>>(img, m, out_or_part,
-                                                                             nsplit, lchunk, err);
+  const dim3 grid(ntri, (unsigned)np, nsplit);
+  if (tf32)
+    k_gram_umma<true><<<grid, kThr, sizeof(USmem), st>>>(img, m, out_or_part, nsplit, lchunk, err);
+  else
+    k_gram_umma<false><<<grid, kThr, sizeof(USmem), st>>>(img, m, out_or_part, nsplit, lchunk, err);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
 }
 
 int rebuild_umma_launch(const cf* img, const cf* W, const PatchMap& m, int64_t np, cf* out,
-                        int direct, cudaStream_t st) {
+                        int direct, cudaStream_t st, bool tf32) {
   if (int rc = umma_prepare()) return rc;
   int* err = umma_err_ptr();
-  k_rebuild_umma<<<dim3((m.n + kTM - 1) / kTM, (m.L + kTN - 1) / kTN, (unsigned)np), kThr,
-                   sizeof(USmem), st>>>(img, W, m, out, direct, err);
+  const dim3 grid((m.n + kTM - 1) / kTM, (m.L + kTN - 1) / kTN, (unsigned)np);
+  if (tf32)
+    k_rebuild_umma<true><<<grid, kThr, sizeof(USmem), st>>>(img, W, m, out, direct, err);
+  else
+    k_rebuild_umma<false><<<grid, kThr, sizeof(USmem), st>>>(img, W, m, out, direct, err);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
 }

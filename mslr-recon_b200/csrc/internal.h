@@ -44,6 +44,10 @@ struct Ctx {
   int64_t K = 0;
   int Ns = 0;
   int form = MSLR_FORM_PLAIN;
+  // tuned-form machinery (specialised SENSE kernels, batched SVST, graph): TUNED and TF32
+  bool tuned() const { return form == MSLR_FORM_TUNED || form == MSLR_FORM_TF32; }
+  // tensor-core mode of the Gram / rebuild products: 0 SIMT FP32, 1 split BF16, 2 TF32
+  int tc_mode() const { return form == MSLR_FORM_TF32 ? 2 : form == MSLR_FORM_TUNED ? 1 : 0; }
   int64_t nvox = 0;
   int device = 0;
   std::vector<ScaleGeom> scales;

@@ -60,10 +60,11 @@ bool mma_supported(const PatchMap& m);
 int tc_prepare();
 
 // gram_umma.cu: the same products on tcgen05 (tuned form, default)
+// (tf32: TF32 operands instead of split BF16, for the TF32 form)
 int gram_umma_launch(const cf* img, const PatchMap& m, int64_t np, cf* out_or_part, int nsplit,
-                     int lchunk, cudaStream_t st);
+                     int lchunk, cudaStream_t st, bool tf32 = false);
 int rebuild_umma_launch(const cf* img, const cf* W, const PatchMap& m, int64_t np, cf* out,
-                        int direct, cudaStream_t st);
+                        int direct, cudaStream_t st, bool tf32 = false);
 int umma_prepare();
 // Reads and clears the tcgen05 kernels' error bits (16: a bounded wait timed out).
 int umma_take_error(int* flags);

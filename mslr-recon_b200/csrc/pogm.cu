@@ -254,7 +254,7 @@ static int pogm_step_body(Ctx* c, cf* X, cudaStream_t st) {
   c->launches += 3;
   // 4. x_i = g_prox(z_i, ζ): patch SVST with threshold ζ·λ_k — scale after
   //    scale in the plain form, all scales batched in the tuned form
-  if (c->form == MSLR_FORM_TUNED) return patch_svst_all(c, c->d_thr, c->d_Z, X, st);
+  if (c->tuned()) return patch_svst_all(c, c->d_thr, c->d_Z, X, st);
   for (int k = 0; k < c->Ns; ++k) {
     if ((rc = patch_svst(c, k, c->d_thr, c->lambdas[k], c->d_Z + k * E, X + k * E, st)))
       return rc;
@@ -269,7 +269,7 @@ static int pogm_step_body(Ctx* c, cf* X, cudaStream_t st) {
 // per-iteration scalars live in device memory (PogmState), so one graph
 // serves every iteration of every run on the same X.
 int pogm_step(Ctx* c, cf* X, cudaStream_t st) {
-  if (c->form != MSLR_FORM_TUNED || !c->use_graph) return pogm_step_body(c, X, st);
+  if (!c->tuned() || !c->use_graph) return pogm_step_body(c, X, st);
   if (!c->gstream) {
     MSLR_CUDA_TRY(cudaStreamCreateWithFlags(&c->gstream, cudaStreamNonBlocking));
     MSLR_CUDA_TRY(cudaEventCreateWithFlags(&c->gev_in, cudaEventDisableTiming));

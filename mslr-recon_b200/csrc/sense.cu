@@ -341,7 +341,7 @@ int sense_setup_tables(Ctx* c) {
   c->nwords = (int)((c->nvox + 31) / 32);
   // tuned form: register-resident kernels when every axis has a fast plan;
   // one frame per chunk so that the chunk's per-coil k-space can stay in L2
-  if (c->form == MSLR_FORM_TUNED) {
+  if (c->tuned()) {
     c->fast = sense_fast_setup(c);
     c->spec = c->fast && sense_spec_setup(c);
   }

@@ -314,7 +314,7 @@ struct WorkPtrs {
 
 // Gram matrices of all patches described by m into w.gram.
 // Tensor cores (tc, tuned form: split-precision BF16 mma) or FP32 SIMT.
-int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit, bool tc,
+int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit, int tc,
               cudaStream_t st, uint64_t* launches) {
   if (launches) *launches += (nsplit > 1 ? 2 : 1);
   const int n = m.n;
@@ -323,8 +323,8 @@ int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
   const int lchunk = (nsplit > 1) ? ((m.L + nsplit - 1) / nsplit + 31) / 32 * 32 : m.L;
   cf* dst = (nsplit > 1) ? w.part : w.gram;
   if (tc && mma_supported(m)) {
-    int rc = use_umma() ? gram_umma_launch(in, m, np, dst, nsplit, lchunk, st)
-                        : gram_mma_launch(in, m, np, dst, nsplit, lchunk, st);
+    int rc = (tc == 2 || use_umma()) ? gram_umma_launch(in, m, np, dst, nsplit, lchunk, st, tc == 2)
+                                     : gram_mma_launch(in, m, np, dst, nsplit, lchunk, st);
     if (rc) return rc;
   } else {
     k_gram<<<dim3(ntri, (unsigned)np, nsplit), 256, 0, st>>>(in, m, dst, nsplit, lchunk);
@@ -336,11 +336,11 @@ int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
 
 // out (image when direct, else per-patch buffer) = rebuild with W in w.gram.
 int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, cf* out,
-                 int direct, bool tc, cudaStream_t st, uint64_t* launches) {
+                 int direct, int tc, cudaStream_t st, uint64_t* launches) {
   if (launches) *launches += 1;
   if (tc && mma_supported(m))
-    return use_umma() ? rebuild_umma_launch(in, w.gram, m, np, out, direct, st)
-                      : rebuild_mma_launch(in, w.gram, m, np, out, direct, st);
+    return (tc == 2 || use_umma()) ? rebuild_umma_launch(in, w.gram, m, np, out, direct, st, tc == 2)
+                                   : rebuild_mma_launch(in, w.gram, m, np, out, direct, st);
   const int n = m.n;
   k_rebuild<<<dim3((n + kTile - 1) / kTile, (m.L + kTile - 1) / kTile, (unsigned)np), 256, 0, st>>>(
       in, w.gram, m, out, direct);
@@ -351,7 +351,7 @@ int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w,
 // W = Ṽ Ṽᴴ for every patch, from the eigen stage's Ṽ (stored conjugated,
 // row-major, in w.zv) into w.gram: the Gram of n × n matrices read as "tall"
 // batch patches, M[a][l] = conj(zv[a·n + l]) = Ṽ[a][l].
-int svst_form_w(const WorkPtrs& w, int n, int64_t np, bool tc, cudaStream_t st,
+int svst_form_w(const WorkPtrs& w, int n, int64_t np, int tc, cudaStream_t st,
                 uint64_t* launches) {
   PatchMap vm{};
   vm.batch = 1;
@@ -367,7 +367,7 @@ int svst_form_w(const WorkPtrs& w, int n, int64_t np, bool tc, cudaStream_t st,
 
 // Gram → eig → W → (rebuild into out or pbuf) for all patches described by m.
 int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
-              const double* thr, int thr_per_patch, double lam, cf* out, int direct, bool tc,
+              const double* thr, int thr_per_patch, double lam, cf* out, int direct, int tc,
               cudaStream_t st, uint64_t* launches) {
   int rc = svst_gram(in, m, np, w, nsplit, tc, st, launches);
   if (rc) return rc;
@@ -499,7 +499,7 @@ int svst_setup(Ctx* c) {
   int rc;
   // plain form: one workspace reused scale after scale; tuned form: one per
   // scale, so that every patch of every scale is in flight in one eigen launch
-  const int nws = (c->form == MSLR_FORM_TUNED) ? c->Ns : 1;
+  const int nws = c->tuned() ? c->Ns : 1;
   c->svw.resize(nws);
   for (int k = 0; k < nws; ++k) {
     const ScaleGeom& g = c->scales[k];
@@ -527,7 +527,7 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
   const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
   const int nsplit = choose_split(g.Np, g.n, g.L);
   WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? s : 0].gram, g.Np, g.n, nsplit);
-  const bool tc = (c->form == MSLR_FORM_TUNED);
+  const int tc = c->tc_mode();
   int rc;
   if (g.partition) {
     cf* dst = img_out;
@@ -569,7 +569,7 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
     const int nsplit = choose_split(g.Np, g.n, g.L);
     ws[k] = carve(c->svw[k].gram, g.Np, g.n, nsplit);
-    if ((rc = svst_gram(Zin + k * E, m, g.Np, ws[k], nsplit, true, st, &c->launches))) return rc;
+    if ((rc = svst_gram(Zin + k * E, m, g.Np, ws[k], nsplit, c->tc_mode(), st, &c->launches))) return rc;
     segs[k].n = g.n;
     segs[k].np = g.Np;
     segs[k].gram = ws[k].gram;
@@ -585,15 +585,18 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     c->launches += (small && big) ? 2 : 1;
   }
   for (int k = 0; k < c->Ns; ++k)
-    if ((rc = svst_form_w(ws[k], c->scales[k].n, c->scales[k].Np, true, st, &c->launches))) return rc;
+    if ((rc = svst_form_w(ws[k], c->scales[k].n, c->scales[k].Np, c->tc_mode(), st, &c->launches)))
+      return rc;
   for (int k = 0; k < c->Ns; ++k) {
     const ScaleGeom& g = c->scales[k];
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
     if (g.partition) {
-      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], Xout + k * E, 1, true, st, &c->launches)))
+      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], Xout + k * E, 1, c->tc_mode(), st,
+                             &c->launches)))
         return rc;
     } else {
-      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], c->d_pbuf, 0, true, st, &c->launches)))
+      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], c->d_pbuf, 0, c->tc_mode(), st,
+                             &c->launches)))
         return rc;
       k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, Xout + k * E);
       MSLR_CUDA_TRY(cudaGetLastError());
@@ -673,7 +676,8 @@ int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* i
                                   cudaMemcpyDeviceToDevice, st));
     src = stage;
   }
-  return svst_core(src, m, batch, w, 1, d_beta, 1, 1.0, out, 1, form == MSLR_FORM_TUNED, st,
+  const int tc = form == MSLR_FORM_TF32 ? 2 : form == MSLR_FORM_TUNED ? 1 : 0;
+  return svst_core(src, m, batch, w, 1, d_beta, 1, 1.0, out, 1, tc, st,
                    nullptr);
 }
 
@@ -744,7 +748,7 @@ int patch_nucnorm_all(Ctx* c, const cf* X, double* reg_out, cudaStream_t st) {
     if ((rc = dalloc(c, (void**)&c->d_zero, sizeof(double)))) return rc;
     MSLR_CUDA_TRY(cudaMemsetAsync(c->d_zero, 0, sizeof(double), st));
   }
-  const bool tc = (c->form == MSLR_FORM_TUNED);
+  const int tc = c->tc_mode();
   std::vector<double> h;
   double reg = 0.0;
   for (int k = 0; k < c->Ns; ++k) {
