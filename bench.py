@@ -32,10 +32,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "metric"
-# DRAM bytes (read + write) of one plane-pass launch (2 frames × 6 coils × 60
-# planes), from the ncu capture summarised in profiles/sense_chunk_kernels_90x90x60.md
-# (cold cache: ncu flushes L2 before the launch, so this is an upper bound)
-PLANE_TRAFFIC_PER_LAUNCH = 47254016 + 2285056
+# DRAM bytes (read + write) per k-space plane of a plane-pass launch, from the
+# ncu capture summarised in profiles/sense_chunk_kernels_90x90x60.md (a launch
+# of 2 frames × 6 coils × 60 planes; cold cache: ncu flushes L2 before the
+# launch, so this is an upper bound; a launch's traffic grows with its planes)
+PLANE_TRAFFIC_PER_PLANE = (47254016 + 2285056) / 720
 # B200 FP32 FMA peak: 148 SMs × 128 lanes × 2 flops × 1.965 GHz (nominal)
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -303,6 +304,7 @@ def main():
         return ctx, X, secs, ck, launches
 
     ctx, X, secs, clocks, launches = device_run(args.form, args.steps, args.warmup)
+    tuning = ctx.tuning()
     value = world * args.steps / secs
 
     # per-phase timing (same stream, CUDA events) for the roofline
@@ -339,14 +341,16 @@ def main():
     if kms:
         phases["normal_op_kernel_ms"] = kms
         phases["normal_op_launches_per_kernel"] = nl
-        planes_per_launch = Nz * min(Nc, 6) * 2   # a chunk: one coil group (6), two frames
+        # a chunk: one coil group × frames per chunk, every kz plane of each
+        planes_per_launch = Nz * min(Nc, tuning["coils_per_group"]) * tuning["frames_per_chunk"]
         byts = RL.plane_pass_bytes(Nx, Ny, planes_per_launch)
         fl = RL.plane_pass_flops(Nx, Ny, planes_per_launch)
         tdom = kms["xy"] / 1e3
         achieved = byts / tdom / 1e9
         roof = {"bound": "hbm", "kernel": "k_xy3 (plane pass: DFT_x, DFT_y, mask, inverse)",
                 "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": PLANE_TRAFFIC_PER_LAUNCH,
+                "frac": achieved / peaks["hbm_gbs"],
+                "traffic": PLANE_TRAFFIC_PER_PLANE * planes_per_launch,
                 "algorithmic_bytes_per_launch": byts, "launch_ms": kms["xy"],
                 "peak_source": peaks["source"],
                 "fp32": {"achieved_tflops": fl / tdom / 1e12, "nominal_peak_tflops": FP32_NOMINAL_TFLOPS,
@@ -416,6 +420,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
                 "config": {"workload": describe(pb),
                            "form": args.form, "parallelism": f"replicas x{world}",
+                           "tuning": tuning,
                            "l2": f"inputs larger than L2 (X is {pb['y'].shape[0] * nvox * 8 * len(pb['patch_sizes']) / 1e9:.1f} GB)",
                            "plain_form_iter_s": plain_ips,
                            "tuned_over_plain": (value / world / plain_ips * world) if plain_ips else None,

@@ -48,6 +48,8 @@ SIGNATURES = {
     "mslr_normal_op": (C.c_int, [_P, _P, _I32, _P, _I32, _P]),
     "mslr_set_graph": (C.c_int, [_P, _I32]),
     "mslr_set_lambdas": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "mslr_autotune": (C.c_int, [_P, _P]),
+    "mslr_get_tuning": (C.c_int, [_P, C.POINTER(_I32), _I32, C.POINTER(_I32)]),
     "mslr_sos_normalize": (C.c_int, [_I32P, _I32, _P, _P, _P]),
     "mslr_sampling": (C.c_int, [_I32P, _I32, _I32, _P, C.POINTER(_I64), _P, _P, _I64, _P]),
     "mslr_prepare": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(C.c_double), _P]),

@@ -252,6 +252,20 @@ class MSLRContext:
                                    y.data_ptr(), idx.data_ptr(), C.byref(sf), _stream_ptr(stream)))
         return smaps, y, idx, float(sf.value)
 
+    def autotune(self, stream=None):
+        """Time the free launch shapes on the bound context and keep the
+        fastest; returns the tuning (see tuning())."""
+        self._chk(lib.mslr_autotune(self._h, _stream_ptr(stream)))
+        return self.tuning()
+
+    def tuning(self):
+        """{'coils_per_group', 'frames_per_chunk', 'gram_splits': [per scale, 0 = heuristic]}"""
+        n = C.c_int32()
+        vals = (C.c_int32 * 64)()
+        self._chk(lib.mslr_get_tuning(self._h, vals, 64, C.byref(n)))
+        v = list(vals[:n.value])
+        return {"coils_per_group": v[0], "frames_per_chunk": v[1], "gram_splits": v[2:]}
+
     def set_lambdas(self, lambdas):
         """Per-scale weights λ_k of g_prox (scripts/reconstruct.jl:164-169, 196-202)."""
         lam = [float(v) for v in lambdas]

@@ -4,6 +4,8 @@
 
 #include <string>
 
+#include <cstdlib>
+#include <vector>
 #include "internal.h"
 #include "patchmap.cuh"
 
@@ -240,6 +242,9 @@ int mslr_bind(mslr_ctx* ctx, const void* smaps, const void* y, const int32_t* id
     return ctx_fail(ctx, fail(MSLR_ERR_ARG, "index_base must be 0 or 1"));
   CTX_RET(ctx, sense_bind(ctx, reinterpret_cast<const cf*>(smaps), reinterpret_cast<const cf*>(y),
                           idx, index_base, reinterpret_cast<cudaStream_t>(stream)));
+  const char* at = std::getenv("MSLR_AUTOTUNE");
+  if (at && std::string(at) == "1" && ctx->tuned())
+    CTX_RET(ctx, autotune(ctx, reinterpret_cast<cudaStream_t>(stream)));
   return MSLR_OK;
 }
 
@@ -405,6 +410,24 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
   CTX_RET(ctx, umma_take_error(&uerr));
   if (uerr)
     return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a tensor-core kernel's wait for its MMAs timed out"));
+  return MSLR_OK;
+}
+
+int mslr_autotune(mslr_ctx* ctx, void* stream) {
+  CTX_CHECK(ctx);
+  NEED_BOUND(ctx);
+  if (!ctx->tuned()) return MSLR_OK;
+  CTX_RET(ctx, autotune(ctx, reinterpret_cast<cudaStream_t>(stream)));
+  return MSLR_OK;
+}
+
+int mslr_get_tuning(const mslr_ctx* ctx, int32_t* values, int32_t cap, int32_t* count) {
+  CTX_CHECK(ctx);
+  if (!count || (cap > 0 && !values)) return fail(MSLR_ERR_ARG, "null argument");
+  std::vector<int32_t> v = {ctx->spec_ch, ctx->spec_fr};
+  for (const auto& g : ctx->scales) v.push_back(g.nsplit_tuned > 0 ? g.nsplit_tuned : 0);
+  *count = (int32_t)v.size();
+  for (int32_t i = 0; i < cap && i < (int32_t)v.size(); ++i) values[i] = v[i];
   return MSLR_OK;
 }
 

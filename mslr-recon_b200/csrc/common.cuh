@@ -62,6 +62,7 @@ struct ScaleGeom {
   // coverage ranges per dim for the gather recombine: for coordinate c in dim d,
   // covering patch indices along d are [lo, hi] (inclusive); -1 if none
   int* d_cover;     // device: per dim, 2*N[d] ints
+  int nsplit_tuned = 0;   // split-K count of the Gram chosen by the autotuner (0: heuristic)
   std::vector<int> h_starts;
 };
 

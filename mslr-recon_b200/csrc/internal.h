@@ -88,6 +88,8 @@ struct Ctx {
   bool xypers = false;    // persistent plane kernel with a prefetch buffer fits
   bool spec = false;      // shape-specialised kernels (sense_spec.cu) exist for N
   int spec_xy_ctas = 0;   // resident CTAs of the specialised plane kernel
+  int spec_ch = 6;        // coils per group of the specialised normal operator (autotuned)
+  int spec_fr = 2;        // frames per chunk (autotuned)
   int spec_zfwd_ctas = 0; // resident CTAs of the specialised forward z kernel
   bool xy_tc = false;     // tensor-core plane pass (DFT products on tcgen05)
   uint32_t* d_dft = nullptr;   // its split-BF16 DFT matrix tiles
@@ -197,6 +199,32 @@ int pogm_step(Ctx* c, cf* X, cudaStream_t st);
 int init_x0(Ctx* c, cf* X, cudaStream_t st);
 int power_iter(Ctx* c, int niter, double tol, double* sigma1, int* iters, cudaStream_t st);
 int set_scalar(double* dst, double v, cudaStream_t st);
+
+// ---- autotuner (api.cu; sense_spec.cu, svst.cu) ---------------------------------
+int tune_sense_chunks(Ctx* c, cudaStream_t st);
+int tune_svst_splits(Ctx* c, cudaStream_t st);
+int autotune(Ctx* c, cudaStream_t st);
+// milliseconds per call of fn(), timed with events on st after one warm-up call
+template <class Fn>
+int time_ms(cudaStream_t st, int reps, float* ms, Fn&& fn) {
+  int rc = fn();
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  MSLR_CUDA_TRY(cudaEventCreate(&e0));
+  MSLR_CUDA_TRY(cudaEventCreate(&e1));
+  cudaEventRecord(e0, st);
+  for (int i = 0; i < reps && !rc; ++i) rc = fn();
+  cudaEventRecord(e1, st);
+  const cudaError_t e = cudaEventSynchronize(e1);
+  float t = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(MSLR_ERR_CUDA, cudaGetErrorString(e));
+  *ms = t / reps;
+  return MSLR_OK;
+}
 
 // ---- set-up of run_recon's inputs (setup.cu) ---------------------------------
 int sos_normalize(const int N[3], int Nc, const cf* in, cf* out, cudaStream_t st);

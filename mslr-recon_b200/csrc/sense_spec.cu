@@ -719,6 +719,16 @@ bool sense_spec_setup(Ctx* c) {
     c->nsm = nsm;
   cudaGetLastError();
   c->spec_xy_ctas = per_sm * c->nsm;
+  // chunk shape (the autotuner may refine it): 6 coils per group, and the most
+  // frames per chunk (up to 4) for which the chunk's k-space and the group's
+  // coil maps, (frames + 1) · 6 images, stay within about 120 MB of the L2
+  c->spec_ch = 6;
+  {
+    const double img = (double)c->nvox * sizeof(cf);
+    int fr = 4;
+    while (fr > 1 && (double)std::min(c->Nc, 6) * (fr + 1) * img > 120e6) --fr;
+    c->spec_fr = fr;
+  }
   c->spec_zfwd_ctas = per_sm_z * c->nsm;
   // tensor-core plane pass only on request (MSLR_XY_PATH=tc): at 90×90 its
   // padded split-BF16 DFT products (12 MMAs of 128×96×16 per K step, four
@@ -756,8 +766,9 @@ int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
   if (!o) return fail(MSLR_ERR_UNSUPPORTED, "no specialised SENSE kernels for this shape");
   float scale = (float)(1.0 / (double)c->nvox);
   const int Nc = c->Nc, Ny = c->N[1], Nz = c->N[2];
-  const int Ch = std::min(Nc, 6);                                  // coils per group
-  const int F = ((int64_t)c->F * Nc >= 2 * (int64_t)Ch) ? 2 : 1;   // frames per chunk
+  const int Ch = std::max(1, std::min(Nc, c->spec_ch));             // coils per group
+  int F = std::max(1, c->spec_fr);                                  // frames per chunk
+  while (F > 1 && (int64_t)F * Ch > (int64_t)c->F * Nc) --F;        // within the k-space buffer
   int nwords = c->nwords;
   const cf* smod = c->d_smaps_mod;
   const uint32_t* mask = c->d_mask;
@@ -822,6 +833,49 @@ int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
   }
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
+}
+
+// Autotuner: coils per group × frames per chunk of the specialised normal
+// operator, timed on the bound context (A'A applied to A'y).  Larger chunks
+// mean fewer launches; the chunk's k-space (Ch·F images) and the group's coil
+// maps should stay in L2.  Clusters of the adjoint z kernel hold Ch CTAs, so
+// Ch ≤ 8.
+int tune_sense_chunks(Ctx* c, cudaStream_t st) {
+  if (!c->spec) return MSLR_OK;
+  const int chs[] = {2, 3, 4, 6, 8};
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  float best = 1e30f;
+  int bch = c->spec_ch, bfr = c->spec_fr;
+  for (int ch : chs) {
+    if (ch > c->Nc) continue;
+    for (int fr = 1; fr <= 4; ++fr) {
+      if ((int64_t)fr * ch > (int64_t)c->F * c->Nc || fr > c->Nt || fr * ch > 24) continue;
+      c->spec_ch = ch;
+      c->spec_fr = fr;
+      float ms = 0.f;
+      int rc = time_ms(st, 2, &ms, [&] { return normal_op_spec(c, c->d_ahy, 1, E, c->d_G, false, st); });
+      if (rc) return rc;
+      if (ms < best) {
+        best = ms;
+        bch = ch;
+        bfr = fr;
+      }
+    }
+  }
+  c->spec_ch = bch;
+  c->spec_fr = bfr;
+  return MSLR_OK;
+}
+
+int autotune(Ctx* c, cudaStream_t st) {
+  int rc = tune_sense_chunks(c, st);
+  if (!rc) rc = tune_svst_splits(c, st);
+  if (c->gexec) {   // the captured iteration holds the old launch shapes
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+    c->gX = nullptr;
+  }
+  return rc;
 }
 
 }  // namespace mslr

@@ -390,6 +390,11 @@ int choose_split(int64_t np, int n, int L) {
   return std::max(1, s);
 }
 
+// the Gram's split-K count of a scale: the autotuner's choice when made
+int split_of(const ScaleGeom& g) {
+  return g.nsplit_tuned > 0 ? g.nsplit_tuned : choose_split(g.Np, g.n, g.L);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -525,7 +530,7 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
                cudaStream_t st) {
   const ScaleGeom& g = c->scales[s];
   const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
-  const int nsplit = choose_split(g.Np, g.n, g.L);
+  const int nsplit = split_of(g);
   WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? s : 0].gram, g.Np, g.n, nsplit);
   const int tc = c->tc_mode();
   int rc;
@@ -567,7 +572,7 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
   for (int k = 0; k < c->Ns; ++k) {
     const ScaleGeom& g = c->scales[k];
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
-    const int nsplit = choose_split(g.Np, g.n, g.L);
+    const int nsplit = split_of(g);
     ws[k] = carve(c->svw[k].gram, g.Np, g.n, nsplit);
     if ((rc = svst_gram(Zin + k * E, m, g.Np, ws[k], nsplit, c->tc_mode(), st, &c->launches))) return rc;
     segs[k].n = g.n;
@@ -908,6 +913,32 @@ int svst_vjp_scale(Ctx* c, int s, const cf* z, const cf* xbar, double beta, cf* 
   double t = 0.0;
   for (double x : hb) t += x;
   *bbar = t;
+  return MSLR_OK;
+}
+
+// Autotuner: split-K count of the Gram of every single-patch scale (the
+// global patch), among the counts its workspace holds, timed on A'y.
+int tune_svst_splits(Ctx* c, cudaStream_t st) {
+  for (size_t k = 0; k < c->scales.size(); ++k) {
+    ScaleGeom& g = c->scales[k];
+    if (g.Np != 1) continue;
+    const int cap = choose_split(g.Np, g.n, g.L);
+    const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
+    float best = 1e30f;
+    int bs = cap;
+    for (int ns = cap; ns >= 1; ns = (ns > 1 && ns / 2 == 0) ? 1 : ns / 2) {
+      WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? k : 0].gram, g.Np, g.n, ns);
+      float ms = 0.f;
+      int rc = time_ms(st, 3, &ms, [&] { return svst_gram(c->d_ahy, m, 1, w, ns, c->tc_mode(), st, nullptr); });
+      if (rc) return rc;
+      if (ms < best) {
+        best = ms;
+        bs = ns;
+      }
+      if (ns == 1) break;
+    }
+    g.nsplit_tuned = bs;
+  }
   return MSLR_OK;
 }
 

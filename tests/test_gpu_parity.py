@@ -355,3 +355,29 @@ def test_mixed_gram_sides_per_iteration(torch, M):
             errs.append(rel(X.cpu().numpy(), traj[i]))
         assert max(errs) < 1e-4, errs
         assert ctx.pogm_restarts() == restarts
+
+
+def test_autotune_keeps_parity(torch, M, small_problem):
+    """The autotuner's choices (SENSE chunk shape, Gram split counts) are valid
+    and the tuned iteration still matches the FP64 oracle."""
+    pb = small_problem
+    Nt, Nc, K = pb["y"].shape
+    niter = 6
+    prob = O.ReconProblem(smaps=pb["smaps"].astype(np.complex128), idx=pb["idx"],
+                          y=pb["y"].astype(np.complex128), patch_sizes=pb["patch_sizes"],
+                          strides=pb["strides"], sigma1=1.0)
+    traj = []
+    _, restarts, _, _ = O.run_recon_arrays(prob, niter, iter_callback=lambda it, xk, r: traj.append(xk.copy()))
+    with M.MSLRContext(pb["N"], Nc, Nt, K, pb["patch_sizes"], pb["strides"], form="tuned") as ctx:
+        ctx.bind(dev(torch, pb["smaps"]), dev(torch, pb["y"]), dev(torch, pb["idx"], torch.int32))
+        t = ctx.autotune()
+        assert t["coils_per_group"] in (2, 3, 4, 6, 8) and 1 <= t["frames_per_chunk"] <= 4
+        assert len(t["gram_splits"]) == len(pb["patch_sizes"])
+        X = ctx.init_x0()
+        ctx.pogm_begin(X, niter, L=1.0)
+        errs = []
+        for i in range(niter):
+            ctx.pogm_step(X)
+            errs.append(rel(X.cpu().numpy(), traj[i]))
+        assert max(errs) < 1e-4, errs
+        assert ctx.pogm_restarts() == restarts
