@@ -34,9 +34,9 @@ sys.path.insert(0, ROOT)
 WORKLOAD = "metric"
 # DRAM bytes (read + write) per k-space plane of a plane-pass launch, from the
 # ncu capture summarised in profiles/sense_chunk_kernels_90x90x60.md (a launch
-# of 2 frames × 6 coils × 60 planes; cold cache: ncu flushes L2 before the
+# of 4 frames × 6 coils × 60 planes; cold cache: ncu flushes L2 before the
 # launch, so this is an upper bound; a launch's traffic grows with its planes)
-PLANE_TRAFFIC_PER_PLANE = (47254016 + 2285056) / 720
+PLANE_TRAFFIC_PER_PLANE = (94088448 + 44334336) / 1440
 # B200 FP32 FMA peak: 148 SMs × 128 lanes × 2 flops × 1.965 GHz (nominal)
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
