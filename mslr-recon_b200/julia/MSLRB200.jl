@@ -20,7 +20,7 @@ module MSLRB200
 using CUDA
 
 export MSLRContext, sense_forward!, sense_adjoint!, dc_cost_grad!, patch_svst!,
-       pogm_run!, power_iter, mslr_lambdas, set_lambdas!, pogm_grad
+       pogm_run!, power_iter, mslr_lambdas, set_lambdas!, pogm_grad, mslr_sampling
 
 const libmslr = get(ENV, "MSLR_LIB", joinpath(@__DIR__, "..", "libmslr.so"))
 
@@ -31,6 +31,7 @@ end
 
 const FORM_PLAIN = Int32(0)
 const FORM_TUNED = Int32(1)
+const FORM_TF32 = Int32(2)
 
 _stream() = CUDA.stream().handle   # cudaStream_t of the task-local stream
 
@@ -68,7 +69,7 @@ function MSLRContext(N, Nc::Integer, Nt::Integer, K::Integer, patch_sizes, strid
                (Ptr{Int32}, Int32, Int32, Int64, Int32, Ptr{Int32}, Ptr{Int32}, Int32,
                 Ptr{Ptr{Cvoid}}),
                Int32[N...], Nc, Nt, K, length(patch_sizes), ps, ss,
-               form === :tuned ? FORM_TUNED : FORM_PLAIN, out)
+               form === :tuned ? FORM_TUNED : form === :tf32 ? FORM_TF32 : FORM_PLAIN, out)
     _check(rc)
     ctx = MSLRContext(out[], Tuple(Int.(N)), Int(Nc), Int(Nt), Int(K), length(patch_sizes), 0)
     finalizer(close, ctx)
@@ -215,6 +216,47 @@ function pogm_grad(ctx::MSLRContext, X_true::CuArray{ComplexF32}, niter::Integer
                  ctx.h, X_true, Int32(niter), Float64(L), Float64(restart_cutoff), Float64(bsig), X,
                  loss, grad, flags, _stream()), ctx.h)
     return loss[], grad, X, Bool.(flags)
+end
+
+"""
+    mslr_sampling(N, Nc, Nt, ksp0) -> K
+
+Samples per frame of the zero-filled k-space `ksp0` `(Nx,Ny,Nz,Nc,Nt)`: the
+mask Ω = ksp0[:,:,:,1,:] .!= 0 with the checks of scripts/reconstruct.jl:113-118
+(`ArgumentError` with the reference's messages otherwise).
+"""
+function mslr_sampling(N, Nc::Integer, Nt::Integer, ksp0::CuArray{ComplexF32})
+    K = Ref{Int64}(0)
+    _check(ccall((:mslr_sampling, libmslr), Cint,
+                 (Ptr{Int32}, Int32, Int32, CuPtr{ComplexF32}, Ref{Int64}, Ptr{Int32}, Ptr{Cvoid},
+                  Int64, Ptr{Cvoid}),
+                 Int32[N...], Int32(Nc), Int32(Nt), ksp0, K, C_NULL, C_NULL, Int64(0), _stream()))
+    return Int(K[])
+end
+
+"""
+    prepare!(ctx, ksp0, smaps_raw) -> (smaps, ksp, idx, scale_factor)
+
+scripts/reconstruct.jl:86-147 on the device: SOS-normalised maps, the samples
+`(K,Nc,Nt)` divided by quantile(abs.(sense_comb(ksp0, smaps)), 0.99), the
+0-based sample indices `(K,Nt)`; the context is bound to them.
+"""
+function prepare!(ctx::MSLRContext, ksp0::CuArray{ComplexF32}, smaps_raw::CuArray{ComplexF32})
+    smaps = similar(smaps_raw)
+    ksp = CuArray{ComplexF32}(undef, ctx.K, ctx.Nc, ctx.Nt)
+    idx = CuArray{Int32}(undef, ctx.K, ctx.Nt)
+    sf = Ref{Float64}(0.0)
+    _check(ccall((:mslr_prepare, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, CuPtr{ComplexF32}, CuPtr{ComplexF32}, CuPtr{ComplexF32},
+                  CuPtr{Int32}, Ref{Float64}, Ptr{Cvoid}),
+                 ctx.h, ksp0, smaps_raw, smaps, ksp, idx, sf, _stream()), ctx.h)
+    return smaps, ksp, idx, sf[]
+end
+
+"""Time the free launch shapes on the bound context and keep the fastest."""
+function autotune!(ctx::MSLRContext)
+    _check(ccall((:mslr_autotune, libmslr), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), ctx.h, _stream()), ctx.h)
+    return ctx
 end
 
 """Ong–Lustig λ_k of scripts/reconstruct.jl:164-169."""
