@@ -58,6 +58,9 @@ static void free_ctx(mslr_ctx* c) {
   if (c->gev_in) cudaEventDestroy(c->gev_in);
   if (c->gev_out) cudaEventDestroy(c->gev_out);
   if (c->gstream) cudaStreamDestroy(c->gstream);
+  for (cudaStream_t x : c->sv_streams) cudaStreamDestroy(x);
+  for (cudaEvent_t e : c->sv_join) cudaEventDestroy(e);
+  if (c->sv_fork) cudaEventDestroy(c->sv_fork);
   if (c->d_nuc) cudaFree(c->d_nuc);
   if (c->d_dft) cudaFree(c->d_dft);
   if (c->d_zero) cudaFree(c->d_zero);

@@ -96,6 +96,10 @@ struct Ctx {
   // graph-captured POGM step (tuned form): captured on a private stream the
   // first time pogm_step sees a given X, replayed afterwards
   cudaStream_t gstream = nullptr;
+  // concurrent per-scale SVST branches (svst.cu): side streams and fork / join events
+  std::vector<cudaStream_t> sv_streams;
+  cudaEvent_t sv_fork = nullptr;
+  std::vector<cudaEvent_t> sv_join;
   cudaEvent_t gev_in = nullptr, gev_out = nullptr;
   cudaGraphExec_t gexec = nullptr;
   const void* gX = nullptr;

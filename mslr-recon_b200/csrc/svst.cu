@@ -554,11 +554,57 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
 }
 
 // g_prox of run_recon (scripts/reconstruct.jl:196-202) for every scale at once:
-// Grams of all scales, one eigen launch over every patch of every scale (the
-// global patch's eigensolve overlaps the local patches'), then the rebuilds.
+// Grams of all scales, one eigen launch per CTA variant over every patch of
+// every scale (the global patch's eigensolve overlaps the local patches'),
+// then the rebuilds.
 // Zin / Xout are (Ns, Nt, Nz, Ny, Nx); threshold of scale k = (*thr_dev)·λ_k.
+//
+// When every scale's patches tile the volume exactly (no shared recombine
+// buffer), the scales instead run as concurrent branches — each its own
+// Gram → eigen → W → rebuild chain — forked from and joined back into st by
+// events (legal inside a stream capture).  The scale with the fewest patches
+// (the global patch) is issued first: its eigensolve takes a slot of the
+// first wave, and its W Gram and rebuild then run on the SMs the larger
+// scale's eigen launch leaves idle in its last wave.
 int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaStream_t st) {
   const int64_t E = (int64_t)c->Nt * c->nvox;
+  bool branches = c->Ns >= 2 && c->Ns <= 8 && c->svw.size() == (size_t)c->Ns;
+  for (const auto& g : c->scales) branches = branches && g.partition;
+  {
+    const char* e = std::getenv("MSLR_SVST_BRANCHES");
+    if (e && std::string(e) == "0") branches = false;
+  }
+  if (branches) {
+    const int ns = c->Ns;
+    if (c->sv_streams.size() < (size_t)ns - 1) {
+      if (!c->sv_fork) MSLR_CUDA_TRY(cudaEventCreateWithFlags(&c->sv_fork, cudaEventDisableTiming));
+      while (c->sv_streams.size() < (size_t)ns - 1) {
+        cudaStream_t x;
+        cudaEvent_t e;
+        MSLR_CUDA_TRY(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        MSLR_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->sv_streams.push_back(x);
+        c->sv_join.push_back(e);
+      }
+    }
+    std::vector<int> order(ns);
+    for (int k = 0; k < ns; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return c->scales[a].Np < c->scales[b].Np; });
+    MSLR_CUDA_TRY(cudaEventRecord(c->sv_fork, st));
+    for (int i = 0; i + 1 < ns; ++i) MSLR_CUDA_TRY(cudaStreamWaitEvent(c->sv_streams[i], c->sv_fork, 0));
+    int rc = MSLR_OK;
+    for (int i = 0; i < ns && !rc; ++i) {   // side branches first, the largest scale on st
+      const int k = order[i];
+      cudaStream_t sk = (i + 1 < ns) ? c->sv_streams[i] : st;
+      rc = patch_svst(c, k, thr_dev, c->lambdas[k], Zin + k * E, Xout + k * E, sk);
+    }
+    for (int i = 0; i + 1 < ns; ++i) {   // join every branch, also after an error
+      cudaEventRecord(c->sv_join[i], c->sv_streams[i]);
+      cudaStreamWaitEvent(st, c->sv_join[i], 0);
+    }
+    return rc;
+  }
   if (c->svw.size() != (size_t)c->Ns) {
     for (int k = 0; k < c->Ns; ++k) {
       int rc = patch_svst(c, k, thr_dev, c->lambdas[k], Zin + k * E, Xout + k * E, st);
