@@ -68,8 +68,49 @@ __global__ void __launch_bounds__(kRedThreads)
   const float alpha = (float)s->alpha, beta = (float)s->beta, gamma = (float)s->gamma;
   const bool sigtest = (s->flags & 1) != 0;
   double r_dot = 0.0, r_g2 = 0.0, r_d2 = 0.0, r_sig = 0.0;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
-       e += (int64_t)gridDim.x * blockDim.x) {
+  // one element: g, and x/u of every scale at offset e
+  auto one = [&](const cf g, const cf* xo, const cf* uo, cf* un, cf* zn) {
+    const cf u = make_float2(xo->x - alpha * g.x, xo->y - alpha * g.y);
+    const cf du = csub(u, *uo);
+    *zn = make_float2(u.x + beta * du.x + gamma * (u.x - xo->x), u.y + beta * du.y + gamma * (u.y - xo->y));
+    *un = u;
+    r_dot += -((double)g.x * du.x - (double)g.y * du.y);
+    r_d2 += (double)du.x * du.x + (double)du.y * du.y;
+  };
+  // pairs of elements with 16-byte accesses when every scale's slab starts on a
+  // 16-byte boundary (E even and the caller's X 16-byte aligned; the library's
+  // own buffers are), else element by element
+  const bool vec = (E % 2 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15u) == 0);
+  const int64_t E2 = vec ? E / 2 : 0;
+  const float4* G4 = reinterpret_cast<const float4*>(G);
+  for (int64_t e2 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e2 < E2;
+       e2 += (int64_t)gridDim.x * blockDim.x) {
+    const float4 g4 = G4[e2];
+    const cf g0 = make_float2(g4.x, g4.y), g1 = make_float2(g4.z, g4.w);
+    r_g2 += (double)g0.x * g0.x + (double)g0.y * g0.y;
+    r_g2 += (double)g1.x * g1.x + (double)g1.y * g1.y;
+    if (sigtest) {
+      float4* GO4 = reinterpret_cast<float4*>(Gold);
+      const float4 go = GO4[e2];
+      r_sig += (double)g0.x * go.x - (double)g0.y * go.y;
+      r_sig += (double)g1.x * go.z - (double)g1.y * go.w;
+      GO4[e2] = g4;
+    }
+    for (int k = 0; k < ns; ++k) {
+      const int64_t o2 = (int64_t)k * (E / 2) + e2;
+      const float4 x4 = reinterpret_cast<const float4*>(X)[o2];
+      const float4 u4 = reinterpret_cast<const float4*>(U)[o2];
+      const cf x0 = make_float2(x4.x, x4.y), x1 = make_float2(x4.z, x4.w);
+      const cf u0 = make_float2(u4.x, u4.y), u1 = make_float2(u4.z, u4.w);
+      cf un0, un1, zn0, zn1;
+      one(g0, &x0, &u0, &un0, &zn0);
+      one(g1, &x1, &u1, &un1, &zn1);
+      reinterpret_cast<float4*>(U)[o2] = make_float4(un0.x, un0.y, un1.x, un1.y);
+      reinterpret_cast<float4*>(Z)[o2] = make_float4(zn0.x, zn0.y, zn1.x, zn1.y);
+    }
+  }
+  for (int64_t e = (vec ? E : 0) + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+       e += (int64_t)gridDim.x * blockDim.x) {   // element by element when not vectorised
     const cf g = G[e];
     r_g2 += (double)g.x * g.x + (double)g.y * g.y;
     if (sigtest) {
@@ -79,16 +120,8 @@ __global__ void __launch_bounds__(kRedThreads)
     }
     for (int k = 0; k < ns; ++k) {
       const int64_t o = (int64_t)k * E + e;
-      const cf xo = X[o];
-      const cf uo = U[o];
-      const cf un = make_float2(xo.x - alpha * g.x, xo.y - alpha * g.y);
-      const cf du = csub(un, uo);
-      const cf zn = make_float2(un.x + beta * du.x + gamma * (un.x - xo.x),
-                                un.y + beta * du.y + gamma * (un.y - xo.y));
-      U[o] = un;
-      Z[o] = zn;
-      r_dot += -((double)g.x * du.x - (double)g.y * du.y);
-      r_d2 += (double)du.x * du.x + (double)du.y * du.y;
+      const cf xo = X[o], uo = U[o];
+      one(g, &xo, &uo, &U[o], &Z[o]);
     }
   }
   double v;

@@ -381,3 +381,37 @@ def test_autotune_keeps_parity(torch, M, small_problem):
             errs.append(rel(X.cpu().numpy(), traj[i]))
         assert max(errs) < 1e-4, errs
         assert ctx.pogm_restarts() == restarts
+
+
+@pytest.mark.parametrize("form", ["plain", "tuned"])
+@pytest.mark.parametrize("N,Nt,bsig", [((9, 9, 9), 5, 0.7), ((12, 10, 8), 6, 0.5)])
+def test_pogm_bsig_and_odd_sizes(torch, M, form, N, Nt, bsig):
+    """POGM with σ decay (bsig < 1: the gradient-sign test and its previous-
+    gradient buffer) on an image × frames count that is odd (element-wise
+    update path) and even (paired update path): every iterate within 1e-4 of
+    the FP64 oracle, identical restart flags."""
+    rng = np.random.default_rng(sum(N) + Nt)
+    Nc = 3
+    nvox = N[0] * N[1] * N[2]
+    K = nvox // 2
+    smaps = rng.standard_normal((Nc, N[2], N[1], N[0])) + 1j * rng.standard_normal((Nc, N[2], N[1], N[0]))
+    smaps /= np.sqrt((np.abs(smaps) ** 2).sum(0))[None]
+    idx = np.stack([np.sort(rng.choice(nvox, K, replace=False)) for _ in range(Nt)]).astype(np.int32)
+    x = (rng.standard_normal((Nt, nvox, 2)) @ rng.standard_normal((2, 1)))[..., 0].reshape(Nt, N[2], N[1], N[0])
+    y = O.sense_forward(x + 0j, smaps, idx) + 0.1 * (rng.standard_normal((Nt, Nc, K)) + 1j * rng.standard_normal((Nt, Nc, K)))
+    ps = [list(N), [3, 3, 2]]
+    prob = O.ReconProblem(smaps=smaps, idx=idx, y=y, patch_sizes=ps, strides=ps, sigma1=1.0)
+    niter = 8
+    traj = []
+    _, restarts, _, _ = O.run_recon_arrays(prob, niter, bsig=bsig,
+                                           iter_callback=lambda it, xk, r: traj.append(xk.copy()))
+    with M.MSLRContext(N, Nc, Nt, K, ps, ps, form=form) as ctx:
+        ctx.bind(dev(torch, smaps), dev(torch, y), dev(torch, idx, torch.int32))
+        X = ctx.init_x0()
+        ctx.pogm_begin(X, niter, L=2.0, bsig=bsig)
+        errs = []
+        for i in range(niter):
+            ctx.pogm_step(X)
+            errs.append(rel(X.cpu().numpy(), traj[i]))
+        assert max(errs) < 1e-4, errs
+        assert ctx.pogm_restarts() == restarts
