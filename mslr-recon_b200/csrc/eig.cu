@@ -91,6 +91,24 @@ __device__ __forceinline__ int sturm_less(const double* d, const double* e2, int
   return cnt;
 }
 
+// sturm_less in FP32 on a copy of T scaled to norm ~1 (d / ‖T‖, e² / ‖T‖²),
+// with the fast reciprocal division: the count is exact for a matrix within a
+// few FP32 roundings of T (the Sturm sequence is backward stable), which is
+// all the first rounds of bracketing need
+__device__ __forceinline__ int sturm_less_f(const float* d, const float* e2, int n, float x) {
+  constexpr float pivmin = 1e-30f;
+  int cnt = 0;
+  float q = d[0] - x;
+  if (fabsf(q) < pivmin) q = -pivmin;
+  cnt += (q < 0.f);
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - __fdividef(e2[i - 1], q);
+    if (fabsf(q) < pivmin) q = -pivmin;
+    cnt += (q < 0.f);
+  }
+  return cnt;
+}
+
 struct Seg {
   int n;
   int64_t first;   // first block of the segment
@@ -418,12 +436,25 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   const double gl = full ? s_bd[0] : fmax(s_bd[0], beta_d * beta_d), gu = s_bd[1],
                pivmin = s_bd[2], tnorm = s_bd[3];
   if (tid == 0) S.rank[ip] = r;
+  // FP32 copy of T scaled by 1/‖T‖ (in the phase-1 vector buffers, free now)
+  const double tsc = fmax(tnorm, 1e-300);
+  float* ddf = reinterpret_cast<float*>(sv);
+  float* e2f = ddf + n;
+  for (int q = tid; q < n; q += kT) {
+    ddf[q] = (float)(dd[q] / tsc);
+    e2f[q] = (float)(ee2[q] / tsc / tsc);
+  }
+  __syncthreads();
   {
     // A group of gsz threads (a power of two, at most a warp) per eigenvalue:
     // each round counts the eigenvalues below gsz evenly spaced interior
     // points of the bracket and keeps the sub-interval holding the
     // eigenvalue, a factor gsz + 1 per round of Sturm sequences instead of
-    // bisection's 2.
+    // bisection's 2.  The first rounds run on the FP32 copy; the bracket is
+    // then widened by 4e-6·‖T‖ (far beyond the FP32 counts' error), checked
+    // with two FP64 counts (the whole interval again if the check fails) and
+    // narrowed in FP64 to 4e-13·‖T‖ — enough for the twisted factorisations'
+    // vectors, whose error scales with |λ̂ − λ| / gap.
     int gsz = 1;
     while (gsz < 32 && 2 * gsz * r <= kT) gsz <<= 1;
     const int e = tid / gsz, sl = tid & (gsz - 1);
@@ -432,7 +463,53 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
       const double frac = (double)(sl + 1) / (double)(gsz + 1);
       double lo = gl, hi = gu;
       bool done = e >= r;
+      if (tnorm > 0.0) {
+        const float fracf = (float)frac;
+        float lof = (float)(gl / tsc), hif = (float)(gu / tsc);
+        bool fdone = done;
+        for (int it = 0; it < 64; ++it) {
+          if (!__any_sync(0xffffffffu, !fdone)) break;
+          const float x = lof + (hif - lof) * fracf;
+          const bool ok = !fdone && x > lof && x < hif;
+          const bool up = ok && sturm_less_f(ddf, e2f, n, x) > kth;
+          float nlo = (ok && !up) ? x : lof;
+          float nhi = (ok && up) ? x : hif;
+          int any = ok ? 1 : 0;
+          for (int o = 1; o < gsz; o <<= 1) {
+            nlo = fmaxf(nlo, __shfl_xor_sync(0xffffffffu, nlo, o));
+            nhi = fminf(nhi, __shfl_xor_sync(0xffffffffu, nhi, o));
+            any |= __shfl_xor_sync(0xffffffffu, any, o);
+          }
+          if (!fdone) {
+            if (!any || !(nlo < nhi)) {
+              fdone = true;
+            } else {
+              lof = nlo;
+              hif = nhi;
+            }
+          }
+        }
+        lo = fmax(gl, ((double)lof - 4e-6) * tsc);
+        hi = fmin(gu, ((double)hif + 4e-6) * tsc);
+        // check the widened bracket in FP64: #{λ < lo} <= kth < #{λ < hi}
+        int c = 0;
+        if (!done) {
+          if (gsz >= 2) c = (sl == 0) ? sturm_less(dd, ee2, n, lo, pivmin)
+                          : (sl == 1) ? sturm_less(dd, ee2, n, hi, pivmin) : 0;
+          else c = sturm_less(dd, ee2, n, lo, pivmin);
+        }
+        const int base = (lane & ~(gsz - 1));
+        const int cl = (gsz >= 2) ? __shfl_sync(0xffffffffu, c, base) : c;
+        int ch = (gsz >= 2) ? __shfl_sync(0xffffffffu, c, base + 1) : 0;
+        if (gsz < 2 && !done) ch = sturm_less(dd, ee2, n, hi, pivmin);
+        if (!done && !(cl <= kth && ch > kth)) {
+          lo = gl;
+          hi = gu;
+        }
+      }
+      const double tol = 4e-13 * tnorm;
       for (int it = 0; it < 200; ++it) {
+        if (!done && !(hi - lo > tol)) done = true;
         if (!__any_sync(0xffffffffu, !done)) break;
         const double x = lo + (hi - lo) * frac;
         const bool ok = !done && x > lo && x < hi;
