@@ -212,6 +212,22 @@ def cpu_sample_iteration(pb, frac_frames: float, frac_patches: float, frac_rows:
     return total, desc, ncores
 
 
+def job_seconds(secs: float, world: int, dist=None, device=None) -> float:
+    """Seconds of the whole job: the maximum of the ranks' timed seconds (the
+    job ends when its slowest replica does).  Every rank gets the result."""
+    if world <= 1:
+        return secs
+    import torch
+    t = torch.tensor([secs], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world: int, steps: int, secs: float) -> float:
+    """Whole-job iterations per second: every replica runs `steps` iterations."""
+    return world * steps / secs
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -297,15 +313,12 @@ def main():
         ck = clocks.stop()
         launches = ctx.launch_count() - n0
         torch.cuda.synchronize()
-        if world > 1:
-            t = torch.tensor([secs], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            secs = float(t.item())
+        secs = job_seconds(secs, world, dist, dev)
         return ctx, X, secs, ck, launches
 
     ctx, X, secs, clocks, launches = device_run(args.form, args.steps, args.warmup)
     tuning = ctx.tuning()
-    value = world * args.steps / secs
+    value = job_value(world, args.steps, secs)
 
     # per-phase timing (same stream, CUDA events) for the roofline
     def ev_time(fn, reps=3):
