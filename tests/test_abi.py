@@ -92,3 +92,37 @@ def test_bad_arguments_rejected_without_gpu(lib):
     b = C.c_size_t()
     assert lib.mslr_svst_batch_workspace(1000, 300, 486, C.byref(b)) == 0 and b.value > 0
     assert lib.mslr_svst_batch_workspace(2000, 2000, 1, C.byref(b)) == 4
+
+
+def test_new_entries_reject_bad_arguments_without_gpu(lib):
+    """The set-up, gradient, weight and tuning entries validate their
+    arguments on the host (MSLR_ERR_ARG = 1) before any device work."""
+    i3 = C.c_int32 * 3
+    P = C.c_void_p
+    K = C.c_int64()
+    # null context
+    assert lib.mslr_set_lambdas(None, (C.c_double * 2)(1.0, 2.0)) == 1
+    assert lib.mslr_get_lambdas(None, (C.c_double * 2)()) == 1
+    assert lib.mslr_autotune(None, None) == 1
+    n = C.c_int32()
+    assert lib.mslr_get_tuning(None, (C.c_int32 * 4)(), 4, C.byref(n)) == 1
+    lib.mslr_pogm_grad.argtypes = [P, P, C.c_int32, C.c_double, C.c_double, C.c_double, P,
+                                   P, P, P, P]
+    assert lib.mslr_pogm_grad(None, None, 5, 2.0, 0.0, 1.0, None, None, None, None, None) == 1
+    lib.mslr_prepare.argtypes = [P, P, P, P, P, P, P, P]
+    assert lib.mslr_prepare(None, None, None, None, None, None, None, None) == 1
+    # set-up entries: bad sizes and null pointers
+    lib.mslr_sos_normalize.argtypes = [P, C.c_int32, P, P, P]
+    assert lib.mslr_sos_normalize(i3(0, 4, 4), 2, P(16), P(16), None) == 1
+    assert lib.mslr_sos_normalize(i3(4, 4, 4), 0, P(16), P(16), None) == 1
+    assert lib.mslr_sos_normalize(i3(4, 4, 4), 2, None, P(16), None) == 1
+    lib.mslr_sampling.argtypes = [P, C.c_int32, C.c_int32, P, P, P, P, C.c_int64, P]
+    assert lib.mslr_sampling(i3(4, 4, 4), 2, 0, P(16), C.byref(K), None, None, 0, None) == 1
+    assert lib.mslr_sampling(i3(4, 4, 4), 2, 3, None, C.byref(K), None, None, 0, None) == 1
+    assert lib.mslr_sampling(i3(4, 4, 4), 2, 3, P(16), None, None, None, 0, None) == 1
+
+
+def test_forms_are_declared():
+    txt = open(HDR).read()
+    for name, value in (("MSLR_FORM_PLAIN", 0), ("MSLR_FORM_TUNED", 1), ("MSLR_FORM_TF32", 2)):
+        assert re.search(rf"#define {name} {value}\b", txt), name
