@@ -198,7 +198,7 @@ int mslr_pogm_begin(mslr_ctx* ctx, void* X, int32_t niter, double L, double rest
                     double bsig, void* stream);
 int mslr_pogm_step(mslr_ctx* ctx, void* X, void* stream);
 
-/* Tuned form only: capture the POGM iteration into a CUDA graph on first use
+/* Tuned and TF32 forms: capture the POGM iteration into a CUDA graph on first use
  * and replay it (enable = 1, the default), or launch its kernels directly
  * (enable = 0).  Both give bit-identical results. */
 int mslr_set_graph(mslr_ctx* ctx, int32_t enable);
