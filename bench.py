@@ -32,10 +32,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "metric"
-# DRAM bytes (read + write) per k-space plane of a plane-pass launch, from the
-# ncu capture summarised in profiles/sense_chunk_kernels_90x90x60.md (a launch
-# of 4 frames × 6 coils × 60 planes; cold cache: ncu flushes L2 before the
-# launch, so this is an upper bound; a launch's traffic grows with its planes)
+# DRAM bytes (read + write) per k-space plane of a plane-pass launch, from an
+# ncu capture of k_xy3 at 90×90×60 (dram__bytes_read.sum + dram__bytes_write.sum
+# of one launch of 4 frames × 6 coils × 60 planes; cold cache: ncu flushes L2
+# before the launch, so this is an upper bound; a launch's traffic grows with
+# its planes)
 PLANE_TRAFFIC_PER_PLANE = (94088448 + 44334336) / 1440
 # B200 FP32 FMA peak: 148 SMs × 128 lanes × 2 flops × 1.965 GHz (nominal)
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
