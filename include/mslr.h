@@ -91,6 +91,9 @@ int mslr_patches2img(const int32_t N[3], int32_t Nt, const int32_t patch[3],
  * back: out_b = U diag(max(S - beta_b, 0)) V^H, zero when ||A_b|| == 0.
  * `betas` is a host array of `batch` thresholds.  The caller provides device
  * scratch of at least mslr_svst_batch_workspace() bytes.  in may equal out.
+ * Synchronises `stream` and reads the call's device error word: when a
+ * tensor-core kernel's bounded wait ran out (mslr_set_wait_limit) the call
+ * returns MSLR_ERR_CUDA and `out` is not valid.
  * ------------------------------------------------------------------------ */
 int mslr_svst_batch_workspace(int32_t m, int32_t n, int32_t batch, size_t* bytes);
 int mslr_svst_batch(int32_t m, int32_t n, int32_t batch, const double* betas,
@@ -113,7 +116,9 @@ int mslr_svst_batch(int32_t m, int32_t n, int32_t batch, const double* betas,
  * address (cudaGetSymbolAddress) with that device current; make that first
  * call before any stream capture.  All calls share the one array, so calls
  * that overlap on the GPU (different streams, or different host threads
- * without ordering) race and corrupt each other's results. */
+ * without ordering) race and corrupt each other's results.  Like
+ * mslr_svst_batch it synchronises `stream` and reports a timed-out bounded
+ * wait as MSLR_ERR_CUDA (its error word lives in the fixed array too). */
 int mslr_svst_batch_noalloc(int32_t m, int32_t n, int32_t batch, const double* betas,
                             const void* in, void* out, void* stream);
 
@@ -191,9 +196,21 @@ int mslr_init_x0(mslr_ctx* ctx, void* X, void* stream);
 int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restart_cutoff,
                   double bsig, uint8_t* restarts_host, void* stream);
 
+/* As mslr_pogm_run, and also fills run_recon's logged costs
+ * (scripts/reconstruct.jl:204-205, saved at :228-230): dc_costs_host[i] and
+ * reg_costs_host[i] (host arrays of niter+1, either may be NULL) receive
+ * mslr_cost's dc_cost and reg_cost of X0 (i = 0) and of x_i after iteration i.
+ * Synchronises `stream` once per iteration. */
+int mslr_pogm_run_costs(mslr_ctx* ctx, void* X, int32_t niter, double L, double restart_cutoff,
+                        double bsig, uint8_t* restarts_host, double* dc_costs_host,
+                        double* reg_costs_host, void* stream);
+
 /* Stepwise POGM: mslr_pogm_begin sets up the state for `niter` iterations
  * from X; each mslr_pogm_step runs exactly one iteration (X holds x_i
- * after it returns, stream-ordered). */
+ * after it returns, stream-ordered).  mslr_pogm_step does not synchronise:
+ * a device-side error of its kernels (a timed-out bounded wait, a
+ * non-finite restart sum) is reported by the next synchronising call on the
+ * context — mslr_pogm_restarts, mslr_sync, mslr_pogm_run. */
 int mslr_pogm_begin(mslr_ctx* ctx, void* X, int32_t niter, double L, double restart_cutoff,
                     double bsig, void* stream);
 int mslr_pogm_step(mslr_ctx* ctx, void* X, void* stream);
@@ -202,8 +219,31 @@ int mslr_pogm_step(mslr_ctx* ctx, void* X, void* stream);
  * and replay it (enable = 1, the default), or launch its kernels directly
  * (enable = 0).  Both give bit-identical results. */
 int mslr_set_graph(mslr_ctx* ctx, int32_t enable);
-/* Restart flags of the iterations run so far (host array of niter+1). */
+/* Restart flags of the iterations run so far (host array of niter+1).
+ * Synchronises `stream` and reports pending device-side errors as mslr_sync. */
 int mslr_pogm_restarts(mslr_ctx* ctx, uint8_t* restarts_host, void* stream);
+
+/* Device-side errors (no counterpart in the reference, whose CUDA.jl calls
+ * throw).  Kernels of a context record errors in the context's own device
+ * error word instead of aborting: MSLR_ERR_NONFINITE for a NaN/Inf restart
+ * sum, MSLR_ERR_CUDA for a bounded wait that ran out (the results written
+ * since the previous check are then not valid).  mslr_sync synchronises
+ * `stream`, reads and clears the word and returns the matching status;
+ * mslr_pogm_run, mslr_pogm_run_costs, mslr_pogm_grad, mslr_pogm_restarts,
+ * mslr_cost, mslr_power_iter and mslr_normal_op_profile do the same before
+ * they return.  The asynchronous entries (mslr_normal_op, mslr_patch_svst,
+ * mslr_pogm_step, the SENSE operators) leave their errors to the next such
+ * call. */
+int mslr_sync(mslr_ctx* ctx, void* stream);
+
+/* Poll count after which a tensor-core kernel's bounded mbarrier wait gives
+ * up (default 2^22, a few tens of milliseconds).  ctx == NULL sets it for the
+ * context-free mslr_svst_batch / mslr_svst_batch_noalloc calls of the whole
+ * process.  A kernel whose wait gives up still waits (with the default
+ * count) for the work it already issued, writes its output tile as zeros,
+ * frees its tensor memory and returns; the call then reports MSLR_ERR_CUDA.
+ * A small value exists to test that path; 0 makes every such wait give up. */
+int mslr_set_wait_limit(mslr_ctx* ctx, int64_t polls);
 
 /* Set-up of run_recon's inputs on the device (scripts/reconstruct.jl:86-147).
  *

@@ -221,6 +221,31 @@ class MSLRContext:
                                     float(restart_cutoff), float(bsig), r, _stream_ptr(stream)))
         return [bool(v) for v in r]
 
+    def pogm_run_costs(self, X: torch.Tensor, niter: int, L: float, restart_cutoff: float = 0.0,
+                       bsig: float = 1.0, stream=None):
+        """pogm_run that also returns run_recon's logged costs: (restarts,
+        dc_costs, reg_costs), each of length niter+1 (X0, then after every
+        iteration; scripts/reconstruct.jl:204-205, 228-230)."""
+        _dev_c64(X, self.x_shape, "X")
+        r = (C.c_uint8 * (niter + 1))()
+        dc = (C.c_double * (niter + 1))()
+        reg = (C.c_double * (niter + 1))()
+        self._chk(lib.mslr_pogm_run_costs(self._h, X.data_ptr(), int(niter), float(L),
+                                          float(restart_cutoff), float(bsig), r, dc, reg,
+                                          _stream_ptr(stream)))
+        self._niter = int(niter)
+        return [bool(v) for v in r], [float(v) for v in dc], [float(v) for v in reg]
+
+    def sync(self, stream=None):
+        """Synchronise the stream and raise any device-side error the
+        context's kernels recorded since the last check."""
+        self._chk(lib.mslr_sync(self._h, _stream_ptr(stream)))
+
+    def set_wait_limit(self, polls: int):
+        """Polls of a tensor-core kernel's bounded wait before it gives up
+        (default 2**22); small values exist to test the time-out path."""
+        self._chk(lib.mslr_set_wait_limit(self._h, int(polls)))
+
     def pogm_begin(self, X, niter, L, restart_cutoff=0.0, bsig=1.0, stream=None):
         _dev_c64(X, self.x_shape, "X")
         self._niter = int(niter)

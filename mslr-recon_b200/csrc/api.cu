@@ -77,6 +77,25 @@ static int ctx_fail(Ctx* c, int code) {
   return code;
 }
 
+int take_error(Ctx* c, cudaStream_t st) {
+  int32_t herr = 0;
+  cudaError_t e = cudaMemcpyAsync(&herr, c->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(MSLR_ERR_CUDA, cudaGetErrorString(e));
+  if (!herr) return MSLR_OK;
+  e = cudaMemsetAsync(c->d_err, 0, sizeof(int32_t), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(MSLR_ERR_CUDA, cudaGetErrorString(e));
+  if (herr & kErrNonfinite) return fail(MSLR_ERR_NONFINITE, "non-finite value in the POGM restart sums");
+  if (herr & kErrMmaWait)
+    return fail(MSLR_ERR_CUDA, "a tensor-core kernel's bounded wait for its MMAs timed out; "
+                               "results since the last check are not valid");
+  if (herr & kErrBulkWait)
+    return fail(MSLR_ERR_CUDA, "a SENSE kernel's bounded wait for a bulk copy timed out; "
+                               "results since the last check are not valid");
+  return fail(MSLR_ERR_CUDA, "device error word " + std::to_string(herr));
+}
+
 }  // namespace mslr
 
 using namespace mslr;
@@ -382,6 +401,7 @@ int mslr_pogm_restarts(mslr_ctx* ctx, uint8_t* restarts_host, void* stream) {
                                   cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
+  CTX_RET(ctx, take_error(ctx, st));
   return MSLR_OK;
 }
 
@@ -401,18 +421,40 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
   }
-  int32_t herr = 0;
-  cudaError_t e = cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
-  if (herr & 4)
-    return ctx_fail(ctx, fail(MSLR_ERR_NONFINITE, "non-finite value in the POGM restart sums"));
-  if (herr & 8)
-    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a device-side wait for a bulk copy timed out"));
-  int uerr = 0;
-  CTX_RET(ctx, umma_take_error(&uerr));
-  if (uerr)
-    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a tensor-core kernel's wait for its MMAs timed out"));
+  CTX_RET(ctx, take_error(ctx, st));
+  return MSLR_OK;
+}
+
+int mslr_pogm_run_costs(mslr_ctx* ctx, void* X, int32_t niter, double L, double restart_cutoff,
+                        double bsig, uint8_t* restarts_host, double* dc_costs_host,
+                        double* reg_costs_host, void* stream) {
+  CTX_CHECK(ctx);
+  NEED_BOUND(ctx);
+  if (!X) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "null argument"));
+  CTX_RET(ctx, check_pogm_args(ctx, niter, L, restart_cutoff, bsig));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  cf* Xc = reinterpret_cast<cf*>(X);
+  // the logger's costs at X0 and after every iteration (scripts/reconstruct.jl:204-205)
+  auto log_costs = [&](int it) -> int {
+    if (dc_costs_host)
+      if (int rc = dc_cost_eval(ctx, Xc, ctx->Ns, &dc_costs_host[it], st)) return rc;
+    if (reg_costs_host)
+      if (int rc = patch_nucnorm_all(ctx, Xc, &reg_costs_host[it], st)) return rc;
+    return MSLR_OK;
+  };
+  CTX_RET(ctx, pogm_begin(ctx, Xc, niter, L, restart_cutoff, bsig, st));
+  CTX_RET(ctx, log_costs(0));
+  for (int i = 0; i < niter; ++i) {
+    CTX_RET(ctx, pogm_step(ctx, Xc, st));
+    CTX_RET(ctx, log_costs(i + 1));
+  }
+  if (restarts_host) {
+    cudaError_t e = cudaMemcpyAsync(restarts_host, ctx->d_restarts, (size_t)niter + 1,
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
+  }
+  CTX_RET(ctx, take_error(ctx, st));
   return MSLR_OK;
 }
 
@@ -497,18 +539,7 @@ int mslr_pogm_grad(mslr_ctx* ctx, const void* X_true, int32_t niter, double L, d
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   CTX_RET(ctx, pogm_grad(ctx, reinterpret_cast<const cf*>(X_true), niter, L, restart_cutoff, bsig,
                          reinterpret_cast<cf*>(X), loss, grad_loglam, restarts_host, st));
-  int32_t herr = 0;
-  cudaError_t e = cudaMemcpyAsync(&herr, ctx->d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
-  if (herr & 4)
-    return ctx_fail(ctx, fail(MSLR_ERR_NONFINITE, "non-finite value in the POGM restart sums"));
-  if (herr & 8)
-    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a device-side wait for a bulk copy timed out"));
-  int uerr = 0;
-  CTX_RET(ctx, umma_take_error(&uerr));
-  if (uerr)
-    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "a tensor-core kernel's wait for its MMAs timed out"));
+  CTX_RET(ctx, take_error(ctx, st));
   return MSLR_OK;
 }
 
@@ -523,6 +554,31 @@ int mslr_cost(mslr_ctx* ctx, const void* X, int32_t ns_in, double* dc_cost, doub
   const cf* Xc = reinterpret_cast<const cf*>(X);
   if (dc_cost) CTX_RET(ctx, dc_cost_eval(ctx, Xc, ns_in, dc_cost, st));
   if (reg_cost) CTX_RET(ctx, patch_nucnorm_all(ctx, Xc, reg_cost, st));
+  CTX_RET(ctx, take_error(ctx, st));
+  return MSLR_OK;
+}
+
+int mslr_sync(mslr_ctx* ctx, void* stream) {
+  CTX_CHECK(ctx);
+  CTX_RET(ctx, take_error(ctx, reinterpret_cast<cudaStream_t>(stream)));
+  return MSLR_OK;
+}
+
+int mslr_set_wait_limit(mslr_ctx* ctx, int64_t polls) {
+  if (polls < 0 || polls > 0x7fffffff) {
+    const int rc = fail(MSLR_ERR_ARG, "polls must be in [0, 2^31 - 1]");
+    return ctx ? ctx_fail(ctx, rc) : rc;
+  }
+  if (!ctx) {
+    set_context_free_polls((int)polls);
+    return MSLR_OK;
+  }
+  if (ctx->wait_polls != (int)polls && ctx->gexec) {
+    // the captured iteration holds the old limit in its kernel arguments
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
+  ctx->wait_polls = (int)polls;
   return MSLR_OK;
 }
 
@@ -546,6 +602,7 @@ int mslr_power_iter(mslr_ctx* ctx, int32_t niter, double tol, double* sigma1, in
   if (!sigma1 || niter <= 0 || !(tol >= 0)) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad argument"));
   int it = 0;
   CTX_RET(ctx, power_iter(ctx, niter, tol, sigma1, &it, reinterpret_cast<cudaStream_t>(stream)));
+  CTX_RET(ctx, take_error(ctx, reinterpret_cast<cudaStream_t>(stream)));
   if (iters_done) *iters_done = it;
   return MSLR_OK;
 }

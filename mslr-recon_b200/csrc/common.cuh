@@ -72,6 +72,27 @@ struct Status {
   std::string msg;
 };
 
+// Bits of a device error word (one int32 per context, or per call of the
+// context-free batched SVST).  Kernels set them with atomicOr; the host reads
+// and clears the word when a call synchronises.
+constexpr int kErrIdxRange = 1;    // bind: a sample index outside the grid
+constexpr int kErrIdxOrder = 2;    // bind: indices not strictly ascending
+constexpr int kErrNonfinite = 4;   // NaN / Inf in the POGM restart sums
+constexpr int kErrBulkWait = 8;    // a SENSE kernel's wait for a bulk copy timed out
+constexpr int kErrMmaWait = 16;    // a tcgen05 kernel's wait for its MMAs timed out
+
+// Default poll count of a bounded mbarrier wait (a few tens of ms on B200).
+constexpr int kWaitPolls = 1 << 22;
+
+// Where a kernel with bounded waits reports a time-out, and how many polls a
+// wait makes before it gives up.  `polls` is settable (mslr_set_wait_limit)
+// so that a test can make a wait run out; the wait that drains in-flight
+// work before a kernel returns always uses kWaitPolls.
+struct DevWait {
+  int* err = nullptr;
+  int polls = kWaitPolls;
+};
+
 }  // namespace mslr
 
 #define MSLR_CUDA_TRY(expr)                                                        \

@@ -1,7 +1,7 @@
 // gram_umma.cu — patch Grams and rebuilds on the 5th-generation tensor cores
 // (tcgen05.mma, accumulators in tensor memory) for the tuned form.
 //
-// Same products as gram_mma.cu, as complex GEMMs over rows with the
+// Patch Grams and rebuilds as complex GEMMs over rows with the
 // contraction index K contiguous:
 //   Gram     G[a][b]      = Σ_l M[a][l] conj(M[b][l])      (A = B = rows of M)
 //   rebuild  M_out[a][l]  = Σ_b W[a][b] M[b][l]            (A = rows of W, B = columns of M)
@@ -28,8 +28,11 @@
 // 8 tiles of 8 KB each).  A stage is reused only after the tcgen05.commit of
 // the MMAs that read it has arrived on the stage's mbarrier.  The epilogue
 // reads the accumulators with tcgen05.ld (warp w: TMEM lanes 32·(w mod 4),
-// columns 64·(w / 4)).  Every wait is bounded; on time-out the kernel stops
-// issuing work, still frees its tensor memory and raises bit 16 of `err`.
+// columns 64·(w / 4)).  Every wait is bounded (DevWait::polls polls).  On a
+// time-out the kernel stops issuing work, thread 0 waits (with the default
+// poll count) for the MMAs it has already committed, the output tile is
+// written as zeros, the tensor memory is freed and kErrMmaWait is raised in
+// the caller's error word.
 #include <cuda_bf16.h>
 
 #include <mutex>
@@ -48,7 +51,6 @@ constexpr int kThr = 256;
 constexpr int kTile = kTM * kKc;  // bf16 per planar tile
 constexpr int kPairs = kTile / 2 / kThr;   // (k, k+1) pairs per thread per operand: 8
 constexpr int kTmemCols = 256;
-constexpr int kErrUmma = 16;
 
 enum { AR_H, AR_L, AI_H, AI_L, BR_H, BR_L, BI_H, BI_L, NOPS };
 
@@ -108,9 +110,9 @@ __device__ __forceinline__ void fence_async_smem() {
 __device__ __forceinline__ void mbar_init(uint64_t* bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(su32(bar)) : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int polls) {
   const unsigned a = su32(bar);
-  for (int it = 0; it < (1 << 22); ++it) {
+  for (int it = 0; it < polls; ++it) {
     unsigned ok;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -312,42 +314,71 @@ __device__ __forceinline__ void issue_chunk(const USmem& s, int st, uint32_t dre
   }
 }
 
-// Main loop shared by both kernels: nch chunks; kofs(c, buf) fills s.kof[buf]
-// for chunk c (threads < 32); returns false on a timed-out wait.
-template <bool GRAM, bool TF, class KOfs>
-__device__ __forceinline__ bool mainloop(USmem& s, int nch, const cf* abase, const cf* bbase,
-                                         bool conjA, bool conjB, bool bSameAsA, const KOfs& kofs) {
-  const int tid = threadIdx.x;
-  Chunk ca, cb;
-  bool ok = true;
-  if (nch > 0) {
-    load_chunk(ca, abase, s.rowA, s.kof[0]);
-    if (!bSameAsA) load_chunk(cb, bbase, s.rowB, s.kof[0]);
+// Commits of thread 0 that it has not yet seen arrive: at most one per stage
+// barrier, since a stage is refilled (and committed again) only after its
+// previous commit has been observed.
+struct Pending {
+  int c0 = -1, c1 = -1;   // chunk committed on bar[0] / bar[1], -1 when none is pending
+  __device__ void committed(int ch) {
+    if (ch & 1) c1 = ch;
+    else c0 = ch;
   }
+  __device__ void observed(int ch) {
+    if (ch & 1) c1 = -1;
+    else c0 = -1;
+  }
+  // After a timed-out wait: thread 0 waits, with the default poll count, for
+  // every commit still pending, so that no MMA reads shared memory or writes
+  // tensor memory after the kernel frees them and returns.
+  __device__ void drain(USmem& s) const {
+    if (c0 >= 0) mbar_wait(&s.bar[0], (unsigned)((c0 >> 1) & 1), kWaitPolls);
+    if (c1 >= 0) mbar_wait(&s.bar[1], (unsigned)((c1 >> 1) & 1), kWaitPolls);
+  }
+};
+
+// Main loop shared by both kernels: nch chunks; kofs(c, buf) fills s.kof[buf]
+// for chunk c (threads < 32); load(c, buf) loads chunk c's operands into
+// registers (A, and B unless bSameAsA); returns false when a wait timed out.
+template <bool GRAM, bool TF, class KOfs, class Load>
+__device__ __forceinline__ bool mainloop(USmem& s, int nch, Chunk& ca, Chunk& cb, bool conjA,
+                                         bool conjB, bool bSameAsA, const KOfs& kofs,
+                                         const Load& load, int polls) {
+  const int tid = threadIdx.x;
+  bool ok = true;
+  Pending pend;
+  if (nch > 0) load(0, 0);
   for (int c = 0; c < nch; ++c) {
     const int st = c & 1;
     if (c + 1 < nch) kofs(c + 1, (c + 1) & 1);
-    if (c >= 2 && ok && !mbar_wait(&s.bar[st], (unsigned)(((c - 2) >> 1) & 1))) ok = false;
+    if (c >= 2 && ok) {
+      if (mbar_wait(&s.bar[st], (unsigned)(((c - 2) >> 1) & 1), polls)) pend.observed(c - 2);
+      else ok = false;
+    }
     if (ok) {
       store_operand<TF>(ca, &s.op[st][0][0], false, conjA);
       if (!bSameAsA) store_operand<TF>(cb, &s.op[st][0][0], true, conjB);
     }
     fence_async_smem();
     __syncthreads();
-    if (c + 1 < nch) {
-      load_chunk(ca, abase, s.rowA, s.kof[(c + 1) & 1]);
-      if (!bSameAsA) load_chunk(cb, bbase, s.rowB, s.kof[(c + 1) & 1]);
-    }
+    if (c + 1 < nch) load(c + 1, (c + 1) & 1);
     if (tid == 0 && ok) {
       tc_fence_after();
       issue_chunk<GRAM, TF>(s, st, s.tmem, s.tmem + kTN, c == 0, bSameAsA);
       umma_commit(&s.bar[st]);
+      pend.committed(c);
     }
     ok = __syncthreads_and(ok);
   }
-  if (nch > 0 && ok && !mbar_wait(&s.bar[(nch - 1) & 1], (unsigned)(((nch - 1) >> 1) & 1))) ok = false;
+  if (nch > 0 && ok) {
+    const int l = nch - 1;
+    if (mbar_wait(&s.bar[l & 1], (unsigned)((l >> 1) & 1), polls)) pend.observed(l);
+    else ok = false;
+  }
+  ok = __syncthreads_and(ok);
+  if (!ok && tid == 0) pend.drain(s);
   tc_fence_after();
-  return __syncthreads_and(ok);
+  __syncthreads();
+  return ok;
 }
 
 __device__ __forceinline__ void tmem_alloc(USmem& s) {
@@ -378,7 +409,7 @@ __device__ __forceinline__ void tmem_free(USmem& s) {
 template <bool TF>
 __global__ void __launch_bounds__(kThr, 1)
     k_gram_umma(const cf* __restrict__ img, PatchMap m, cf* __restrict__ out, int nsplit,
-                int lchunk, int* __restrict__ err) {
+                int lchunk, DevWait dw) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   USmem& s = *reinterpret_cast<USmem*>(smraw);
   int t = blockIdx.x, ta = 0;
@@ -414,16 +445,25 @@ __global__ void __launch_bounds__(kThr, 1)
   tc_fence_after();
   const cf* base = img + org;
   const bool cj = m.tall != 0;
-  const bool ok = mainloop<true, TF>(s, nch, base, base, cj, cj, diag, kofs);
+  Chunk ca, cb;
+  auto load = [&](int c, int buf) {
+    (void)c;
+    load_chunk(ca, base, s.rowA, s.kof[buf]);
+    if (!diag) load_chunk(cb, base, s.rowB, s.kof[buf]);
+  };
+  const bool ok = mainloop<true, TF>(s, nch, ca, cb, cj, cj, diag, kofs, load, dw.polls);
   cf* G = out + ((nsplit > 1) ? (int64_t)split * n * n : ip * (int64_t)n * n);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int a = a0 + (warp & 3) * 32 + lane;
-  if (ok) {
+  // on a time-out the tile is written as zeros (a zero Gram: the eigen stage
+  // then finds no singular value above the threshold) and the error raised
+  if (!ok && threadIdx.x == 0 && dw.err) atomicOr(dw.err, kErrMmaWait);
+  {
     for (int cb = 0; cb < 4; ++cb) {
       const int col = (warp >> 2) * 64 + cb * 16;
       const uint32_t taddr = s.tmem + ((uint32_t)((warp & 3) * 32) << 16) + col;
       float re[16], im[16];
-      if (nch > 0) {
+      if (ok && nch > 0) {
         tmem_ld16(taddr, re);
         tmem_ld16(taddr + kTN, im);
       } else {
@@ -442,8 +482,6 @@ __global__ void __launch_bounds__(kThr, 1)
         }
       }
     }
-  } else if (threadIdx.x == 0 && err) {
-    atomicOr(err, kErrUmma);
   }
   tmem_free(s);
 }
@@ -452,7 +490,7 @@ __global__ void __launch_bounds__(kThr, 1)
 template <bool TF>
 __global__ void __launch_bounds__(kThr, 1)
     k_rebuild_umma(const cf* __restrict__ img, const cf* __restrict__ W, PatchMap m,
-                   cf* __restrict__ out, int direct, int* __restrict__ err) {
+                   cf* __restrict__ out, int direct, DevWait dw) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   USmem& s = *reinterpret_cast<USmem*>(smraw);
   const int a0 = blockIdx.x * kTM, l0 = blockIdx.y * kTN;
@@ -480,67 +518,41 @@ __global__ void __launch_bounds__(kThr, 1)
   kofs(0, 0);
   __syncthreads();
   tc_fence_after();
-  // A's element (a, b) is at Wp[a·n + b]; B's element (l, b) at org + rowB[l] + kof[b].
-  // mainloop applies one kof table to both, so A reads through a second table
-  // built from the same b: store A's K offsets (b itself) in the row table's
-  // place by addressing W with row = a·n and K offset = b.
-  const bool ok = [&]() {
-    Chunk ca, cb;
-    bool good = true;
-    auto kA = [&](int c, int i) { const int b = c * kKc + i; return b < n ? b : -1; };
-    auto loadA = [&](int c) {
+  // A's element (a, b) is at Wp[a·n + b] (rows a·n in rowA, K offset b itself);
+  // B's element (l, b) at org + rowB[l] + kof[b].
+  Chunk ca, cb;
+  auto load = [&](int c, int buf) {
 #pragma unroll
-      for (int i = 0; i < kPairs; ++i) {
-        int r, k;
-        pair_rk(i, r, k);
-        const int ro = s.rowA[r];
+    for (int i = 0; i < kPairs; ++i) {
+      int r, k;
+      pair_rk(i, r, k);
+      const int ro = s.rowA[r];
 #pragma unroll
-        for (int d = 0; d < 2; ++d) {
-          const int ko = kA(c, k + d);
-          ca.v[i][d] = (ro >= 0 && ko >= 0) ? __ldg(Wp + ro + ko) : make_float2(0.f, 0.f);
-        }
+      for (int d = 0; d < 2; ++d) {
+        const int b = c * kKc + k + d;
+        ca.v[i][d] = (ro >= 0 && b < n) ? __ldg(Wp + ro + b) : make_float2(0.f, 0.f);
       }
-    };
-    if (nch > 0) {
-      loadA(0);
-      load_chunk(cb, img + org, s.rowB, s.kof[0]);
     }
-    for (int c = 0; c < nch; ++c) {
-      const int st = c & 1;
-      if (c + 1 < nch) kofs(c + 1, (c + 1) & 1);
-      if (c >= 2 && good && !mbar_wait(&s.bar[st], (unsigned)(((c - 2) >> 1) & 1))) good = false;
-      if (good) {
-        store_operand<TF>(ca, &s.op[st][0][0], false, true);
-        store_operand<TF>(cb, &s.op[st][0][0], true, m.tall != 0);
-      }
-      fence_async_smem();
-      __syncthreads();
-      if (c + 1 < nch) {
-        loadA(c + 1);
-        load_chunk(cb, img + org, s.rowB, s.kof[(c + 1) & 1]);
-      }
-      if (threadIdx.x == 0 && good) {
-        tc_fence_after();
-        issue_chunk<false, TF>(s, st, s.tmem, s.tmem + kTN, c == 0, false);
-        umma_commit(&s.bar[st]);
-      }
-      good = __syncthreads_and(good);
-    }
-    if (nch > 0 && good && !mbar_wait(&s.bar[(nch - 1) & 1], (unsigned)(((nch - 1) >> 1) & 1)))
-      good = false;
-    tc_fence_after();
-    return (bool)__syncthreads_and(good);
-  }();
+    load_chunk(cb, img + org, s.rowB, s.kof[buf]);
+  };
+  const bool ok = mainloop<false, TF>(s, nch, ca, cb, true, m.tall != 0, false, kofs, load, dw.polls);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int a = a0 + (warp & 3) * 32 + lane;
-  if (ok) {
+  // on a time-out the output tile is written as zeros and the error raised
+  if (!ok && threadIdx.x == 0 && dw.err) atomicOr(dw.err, kErrMmaWait);
+  {
     const int64_t offa = (a < n && !m.tall) ? patch_off(m, a) : 0;
     for (int cb = 0; cb < 4; ++cb) {
       const int col = (warp >> 2) * 64 + cb * 16;
       const uint32_t taddr = s.tmem + ((uint32_t)((warp & 3) * 32) << 16) + col;
       float re[16], im[16];
-      tmem_ld16(taddr, re);
-      tmem_ld16(taddr + kTN, im);
+      if (ok && nch > 0) {
+        tmem_ld16(taddr, re);
+        tmem_ld16(taddr + kTN, im);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) re[j] = im[j] = 0.f;
+      }
       if (a < n) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
@@ -558,44 +570,16 @@ __global__ void __launch_bounds__(kThr, 1)
         }
       }
     }
-  } else if (threadIdx.x == 0 && err) {
-    atomicOr(err, kErrUmma);
   }
   tmem_free(s);
 }
 
 }  // namespace
 
-// Error word of the tcgen05 kernels (bit 16: a bounded wait timed out),
-// read and cleared by umma_take_error().
-__device__ int g_umma_err = 0;
-
-static int* umma_err_ptr() {
-  static std::mutex mu;
-  static int* ptr[64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64) return nullptr;
-  std::lock_guard<std::mutex> lk(mu);
-  if (!ptr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_umma_err) != cudaSuccess) {
-      cudaGetLastError();
-      return nullptr;
-    }
-    ptr[dev] = static_cast<int*>(p);
-  }
-  return ptr[dev];
-}
-
-int umma_take_error(int* flags) {
-  int h = 0;
-  MSLR_CUDA_TRY(cudaMemcpyFromSymbol(&h, g_umma_err, sizeof(int)));
-  if (h) {
-    const int z = 0;
-    MSLR_CUDA_TRY(cudaMemcpyToSymbol(g_umma_err, &z, sizeof(int)));
-  }
-  *flags = h;
-  return MSLR_OK;
+// The 32-bit row and K offset tables of the tcgen05 kernels cover this map.
+bool umma_supported(const PatchMap& m) {
+  const int64_t span = m.batch ? m.mstride : (int64_t)m.Nt * m.nvox;
+  return span < (int64_t)0x7fffffff && (int64_t)m.n * m.n < (int64_t)0x7fffffff;
 }
 
 int umma_prepare() {
@@ -618,29 +602,27 @@ int umma_prepare() {
 }
 
 int gram_umma_launch(const cf* img, const PatchMap& m, int64_t np, cf* out_or_part, int nsplit,
-                     int lchunk, cudaStream_t st, bool tf32) {
+                     int lchunk, const DevWait& dw, cudaStream_t st, bool tf32) {
   if (int rc = umma_prepare()) return rc;
-  int* err = umma_err_ptr();
   const int T = (m.n + kTM - 1) / kTM;
   const int ntri = T * (T + 1) / 2;
   const dim3 grid(ntri, (unsigned)np, nsplit);
   if (tf32)
-    k_gram_umma<true><<<grid, kThr, sizeof(USmem), st>>>(img, m, out_or_part, nsplit, lchunk, err);
+    k_gram_umma<true><<<grid, kThr, sizeof(USmem), st>>>(img, m, out_or_part, nsplit, lchunk, dw);
   else
-    k_gram_umma<false><<<grid, kThr, sizeof(USmem), st>>>(img, m, out_or_part, nsplit, lchunk, err);
+    k_gram_umma<false><<<grid, kThr, sizeof(USmem), st>>>(img, m, out_or_part, nsplit, lchunk, dw);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
 }
 
 int rebuild_umma_launch(const cf* img, const cf* W, const PatchMap& m, int64_t np, cf* out,
-                        int direct, cudaStream_t st, bool tf32) {
+                        int direct, const DevWait& dw, cudaStream_t st, bool tf32) {
   if (int rc = umma_prepare()) return rc;
-  int* err = umma_err_ptr();
   const dim3 grid((m.n + kTM - 1) / kTM, (m.L + kTN - 1) / kTN, (unsigned)np);
   if (tf32)
-    k_rebuild_umma<true><<<grid, kThr, sizeof(USmem), st>>>(img, W, m, out, direct, err);
+    k_rebuild_umma<true><<<grid, kThr, sizeof(USmem), st>>>(img, W, m, out, direct, dw);
   else
-    k_rebuild_umma<false><<<grid, kThr, sizeof(USmem), st>>>(img, W, m, out, direct, err);
+    k_rebuild_umma<false><<<grid, kThr, sizeof(USmem), st>>>(img, W, m, out, direct, dw);
   MSLR_CUDA_TRY(cudaGetLastError());
   return MSLR_OK;
 }

@@ -122,7 +122,8 @@ struct Ctx {
   uint8_t* d_restarts = nullptr;  // niter+1
   int restarts_cap = 0;
   double* d_thr = nullptr;    // device threshold multiplier (ζ for POGM, β for standalone)
-  int32_t* d_err = nullptr;   // device error word
+  int32_t* d_err = nullptr;   // device error word (kErr* bits), read and cleared by take_error
+  int wait_polls = kWaitPolls; // polls of a bounded wait in this context's tcgen05 kernels
   bool pogm_ready = false;
 
   // SVST
@@ -138,6 +139,21 @@ struct Ctx {
 
 // ---- device memory helper -------------------------------------------------
 int dalloc(Ctx* c, void** p, size_t bytes);
+
+// ---- device-side errors (api.cu, svst.cu) -----------------------------------
+// Error word and wait limit of a context's kernels.
+inline DevWait ctx_wait(Ctx* c) {
+  DevWait w;
+  w.err = c->d_err;
+  w.polls = c->wait_polls;
+  return w;
+}
+// Synchronises st, reads and clears the context's error word; returns the
+// status its bits map to (MSLR_OK when none is set).
+int take_error(Ctx* c, cudaStream_t st);
+// Poll count of the bounded waits of the context-free batched SVST calls.
+int context_free_polls();
+void set_context_free_polls(int polls);
 
 // ---- sense.cu ----------------------------------------------------------------
 int sense_setup_tables(Ctx* c);   // twiddles, phases, plans (create time)

@@ -53,26 +53,14 @@ __device__ __forceinline__ cf m_elem(const PatchMap& m, const cf* __restrict__ i
 }
 
 
-// gram_mma.cu: split-precision BF16 tensor-core Gram and rebuild (tuned form).
-// mma_supported: the 32-bit offset tables of those kernels cover this map.
-bool mma_supported(const PatchMap& m);
-// Opt the tensor-core kernels into their shared memory on the current device.
-int tc_prepare();
-
-// gram_umma.cu: the same products on tcgen05 (tuned form, default)
-// (tf32: TF32 operands instead of split BF16, for the TF32 form)
+// gram_umma.cu: split-precision BF16 (or TF32) patch Grams and rebuilds on
+// tcgen05 for the tuned and TF32 forms.
+// umma_supported: the 32-bit offset tables of those kernels cover this map.
+bool umma_supported(const PatchMap& m);
 int gram_umma_launch(const cf* img, const PatchMap& m, int64_t np, cf* out_or_part, int nsplit,
-                     int lchunk, cudaStream_t st, bool tf32 = false);
+                     int lchunk, const DevWait& dw, cudaStream_t st, bool tf32 = false);
 int rebuild_umma_launch(const cf* img, const cf* W, const PatchMap& m, int64_t np, cf* out,
-                        int direct, cudaStream_t st, bool tf32 = false);
+                        int direct, const DevWait& dw, cudaStream_t st, bool tf32 = false);
 int umma_prepare();
-// Reads and clears the tcgen05 kernels' error bits (16: a bounded wait timed out).
-int umma_take_error(int* flags);
-// Tensor-core path of the tuned form: tcgen05 unless MSLR_TENSOR_PATH=mma.
-bool use_umma();
-int gram_mma_launch(const cf* img, const PatchMap& m, int64_t np, cf* out_or_part, int nsplit,
-                    int lchunk, cudaStream_t st);
-int rebuild_mma_launch(const cf* img, const cf* W, const PatchMap& m, int64_t np, cf* out,
-                       int direct, cudaStream_t st);
 
 }  // namespace mslr

@@ -150,7 +150,7 @@ __global__ void k_pogm_finish(PogmState* s, const double* __restrict__ part, int
   const double dnorm = sqrt(tot[2]);
   const double sigdot = (double)ns * tot[3];
   for (int q = 0; q < 4; ++q) s->red[q] = tot[q];
-  if (!isfinite(dot) || !isfinite(gnorm) || !isfinite(dnorm)) atomicOr(err, 4);
+  if (!isfinite(dot) || !isfinite(gnorm) || !isfinite(dnorm)) atomicOr(err, kErrNonfinite);
   int restart = 0;
   double tnew = s->tnew;
   if (dot <= s->restart_cutoff * gnorm * dnorm) {

@@ -44,7 +44,7 @@ using spec::Ax2;
 using spec::GmC;
 using spec::SmC;
 
-constexpr int kErrWait = 8;
+constexpr int kErrWait = kErrBulkWait;
 
 // A copy of p the compiler cannot see through: loads through it are not
 // hoisted out of the surrounding loop (which would pin every twiddle of every

@@ -21,6 +21,7 @@
 // count, clamped to 1 (src/recon.jl:113-124).
 #include <algorithm>
 #include <cmath>
+#include <atomic>
 #include <mutex>
 
 #include <cstdlib>
@@ -31,14 +32,11 @@
 
 namespace mslr {
 
-bool use_umma() {
-  static const bool v = [] {
-    const char* e = std::getenv("MSLR_TENSOR_PATH");
-    return !(e && std::string(e) == "mma");
-  }();
-  return v;
-}
-
+// Poll count of the bounded waits in context-free calls (mslr_svst_batch,
+// mslr_svst_batch_noalloc); contexts carry their own (Ctx::wait_polls).
+static std::atomic<int> g_free_polls{kWaitPolls};
+int context_free_polls() { return g_free_polls.load(); }
+void set_context_free_polls(int polls) { g_free_polls.store(polls); }
 
 namespace {
 
@@ -315,17 +313,15 @@ struct WorkPtrs {
 // Gram matrices of all patches described by m into w.gram.
 // Tensor cores (tc, tuned form: split-precision BF16 mma) or FP32 SIMT.
 int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit, int tc,
-              cudaStream_t st, uint64_t* launches) {
+              const DevWait& dw, cudaStream_t st, uint64_t* launches) {
   if (launches) *launches += (nsplit > 1 ? 2 : 1);
   const int n = m.n;
   const int T = (n + kTile - 1) / kTile;
   const int ntri = T * (T + 1) / 2;
   const int lchunk = (nsplit > 1) ? ((m.L + nsplit - 1) / nsplit + 31) / 32 * 32 : m.L;
   cf* dst = (nsplit > 1) ? w.part : w.gram;
-  if (tc && mma_supported(m)) {
-    int rc = (tc == 2 || use_umma()) ? gram_umma_launch(in, m, np, dst, nsplit, lchunk, st, tc == 2)
-                                     : gram_mma_launch(in, m, np, dst, nsplit, lchunk, st);
-    if (rc) return rc;
+  if (tc && umma_supported(m)) {
+    if (int rc = gram_umma_launch(in, m, np, dst, nsplit, lchunk, dw, st, tc == 2)) return rc;
   } else {
     k_gram<<<dim3(ntri, (unsigned)np, nsplit), 256, 0, st>>>(in, m, dst, nsplit, lchunk);
   }
@@ -336,11 +332,10 @@ int svst_gram(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
 
 // out (image when direct, else per-patch buffer) = rebuild with W in w.gram.
 int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, cf* out,
-                 int direct, int tc, cudaStream_t st, uint64_t* launches) {
+                 int direct, int tc, const DevWait& dw, cudaStream_t st, uint64_t* launches) {
   if (launches) *launches += 1;
-  if (tc && mma_supported(m))
-    return (tc == 2 || use_umma()) ? rebuild_umma_launch(in, w.gram, m, np, out, direct, st, tc == 2)
-                                   : rebuild_mma_launch(in, w.gram, m, np, out, direct, st);
+  if (tc && umma_supported(m))
+    return rebuild_umma_launch(in, w.gram, m, np, out, direct, dw, st, tc == 2);
   const int n = m.n;
   k_rebuild<<<dim3((n + kTile - 1) / kTile, (m.L + kTile - 1) / kTile, (unsigned)np), 256, 0, st>>>(
       in, w.gram, m, out, direct);
@@ -351,7 +346,7 @@ int svst_rebuild(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w,
 // W = Ṽ Ṽᴴ for every patch, from the eigen stage's Ṽ (stored conjugated,
 // row-major, in w.zv) into w.gram: the Gram of n × n matrices read as "tall"
 // batch patches, M[a][l] = conj(zv[a·n + l]) = Ṽ[a][l].
-int svst_form_w(const WorkPtrs& w, int n, int64_t np, int tc, cudaStream_t st,
+int svst_form_w(const WorkPtrs& w, int n, int64_t np, int tc, const DevWait& dw, cudaStream_t st,
                 uint64_t* launches) {
   PatchMap vm{};
   vm.batch = 1;
@@ -362,21 +357,21 @@ int svst_form_w(const WorkPtrs& w, int n, int64_t np, int tc, cudaStream_t st,
   vm.L = n;
   vm.nvox = n;
   vm.mstride = (int64_t)n * n;
-  return svst_gram(reinterpret_cast<const cf*>(w.zv), vm, np, w, 1, tc, st, launches);
+  return svst_gram(reinterpret_cast<const cf*>(w.zv), vm, np, w, 1, tc, dw, st, launches);
 }
 
 // Gram → eig → W → (rebuild into out or pbuf) for all patches described by m.
 int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
               const double* thr, int thr_per_patch, double lam, cf* out, int direct, int tc,
-              cudaStream_t st, uint64_t* launches) {
-  int rc = svst_gram(in, m, np, w, nsplit, tc, st, launches);
+              const DevWait& dw, cudaStream_t st, uint64_t* launches) {
+  int rc = svst_gram(in, m, np, w, nsplit, tc, dw, st, launches);
   if (rc) return rc;
   if (launches) *launches += 1;
   rc = eig2_launch(m.n, np, w.gram, reinterpret_cast<cf*>(w.zv), reinterpret_cast<float*>(w.aux),
                    w.rank, thr, thr_per_patch, lam, st);
   if (rc) return rc;
-  if ((rc = svst_form_w(w, m.n, np, tc, st, launches))) return rc;
-  return svst_rebuild(in, m, np, w, out, direct, tc, st, launches);
+  if ((rc = svst_form_w(w, m.n, np, tc, dw, st, launches))) return rc;
+  return svst_rebuild(in, m, np, w, out, direct, tc, dw, st, launches);
 }
 
 // Split-K partial Grams are laid out one n × n block per split, so only a
@@ -521,8 +516,7 @@ int svst_setup(Ctx* c) {
   if ((rc = dalloc(c, (void**)&c->d_img_tmp, (size_t)c->Nt * c->nvox * sizeof(cf)))) return rc;
   int nmax = 1;
   for (auto& g : c->scales) nmax = std::max(nmax, g.n);
-  if ((rc = tc_prepare())) return rc;   // before any graph capture of the iteration
-  if ((rc = umma_prepare())) return rc;
+  if ((rc = umma_prepare())) return rc;   // before any graph capture of the iteration
   return eig2_prepare(nmax);
 }
 
@@ -537,13 +531,14 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
   if (g.partition) {
     cf* dst = img_out;
     if (img_in == img_out) dst = c->d_img_tmp;   // Gram/rebuild read the input throughout
-    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, dst, 1, tc, st, &c->launches)))
+    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, dst, 1, tc, ctx_wait(c), st,
+                        &c->launches)))
       return rc;
     if (dst != img_out)
       MSLR_CUDA_TRY(cudaMemcpyAsync(img_out, dst, (size_t)c->Nt * c->nvox * sizeof(cf),
                                     cudaMemcpyDeviceToDevice, st));
   } else {
-    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, c->d_pbuf, 0, tc, st,
+    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, c->d_pbuf, 0, tc, ctx_wait(c), st,
                         &c->launches)))
       return rc;
     k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, img_out);
@@ -620,7 +615,8 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
     const int nsplit = split_of(g);
     ws[k] = carve(c->svw[k].gram, g.Np, g.n, nsplit);
-    if ((rc = svst_gram(Zin + k * E, m, g.Np, ws[k], nsplit, c->tc_mode(), st, &c->launches))) return rc;
+    if ((rc = svst_gram(Zin + k * E, m, g.Np, ws[k], nsplit, c->tc_mode(), ctx_wait(c), st, &c->launches)))
+      return rc;
     segs[k].n = g.n;
     segs[k].np = g.Np;
     segs[k].gram = ws[k].gram;
@@ -636,17 +632,18 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     c->launches += (small && big) ? 2 : 1;
   }
   for (int k = 0; k < c->Ns; ++k)
-    if ((rc = svst_form_w(ws[k], c->scales[k].n, c->scales[k].Np, c->tc_mode(), st, &c->launches)))
+    if ((rc = svst_form_w(ws[k], c->scales[k].n, c->scales[k].Np, c->tc_mode(), ctx_wait(c), st,
+                          &c->launches)))
       return rc;
   for (int k = 0; k < c->Ns; ++k) {
     const ScaleGeom& g = c->scales[k];
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
     if (g.partition) {
-      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], Xout + k * E, 1, c->tc_mode(), st,
+      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], Xout + k * E, 1, c->tc_mode(), ctx_wait(c), st,
                              &c->launches)))
         return rc;
     } else {
-      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], c->d_pbuf, 0, c->tc_mode(), st,
+      if ((rc = svst_rebuild(Zin + k * E, m, g.Np, ws[k], c->d_pbuf, 0, c->tc_mode(), ctx_wait(c), st,
                              &c->launches)))
         return rc;
       k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, Xout + k * E);
@@ -684,12 +681,17 @@ int patches_op(const int N[3], int Nt, const int ps[3], const int ss[3], const c
   return MSLR_OK;
 }
 
+// Workspace of the batched SVST: the eigen-stage work arrays, the thresholds,
+// an error word and a staging copy of the input (for in == out).
 size_t svst_batch_bytes(int mrows, int ncols, int batch) {
   const int n = std::min(mrows, ncols);
-  return eig_work_bytes(batch, n, 1) + (size_t)batch * sizeof(double) + 256 +
+  return eig_work_bytes(batch, n, 1) + (size_t)batch * sizeof(double) + 256 + 256 +
          (size_t)batch * mrows * ncols * sizeof(cf) + 256;
 }
 
+// Runs every stage on st, then synchronises st and reads the call's error
+// word: a bounded wait that ran out in a tensor-core kernel makes the call
+// return MSLR_ERR_CUDA, and `out` is then not valid.
 int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* in, cf* out,
                void* ws, size_t ws_bytes, int form, cudaStream_t st) {
   const int n = std::min(mrows, ncols);
@@ -700,8 +702,11 @@ int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* i
   tail = reinterpret_cast<unsigned char*>(((uintptr_t)tail + 255) & ~(uintptr_t)255);
   double* d_beta = reinterpret_cast<double*>(tail);
   tail += ((size_t)batch * sizeof(double) + 255) & ~(size_t)255;
+  int* d_err = reinterpret_cast<int*>(tail);
+  tail += 256;
   cf* stage = reinterpret_cast<cf*>(tail);
   MSLR_CUDA_TRY(cudaMemcpyAsync(d_beta, betas, batch * sizeof(double), cudaMemcpyHostToDevice, st));
+  MSLR_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   PatchMap m;
   m.Nx = mrows;
   m.Ny = 1;
@@ -728,8 +733,17 @@ int svst_batch(int mrows, int ncols, int batch, const double* betas, const cf* i
     src = stage;
   }
   const int tc = form == MSLR_FORM_TF32 ? 2 : form == MSLR_FORM_TUNED ? 1 : 0;
-  return svst_core(src, m, batch, w, 1, d_beta, 1, 1.0, out, 1, tc, st,
-                   nullptr);
+  DevWait dw;
+  dw.err = d_err;
+  dw.polls = context_free_polls();
+  if ((rc = svst_core(src, m, batch, w, 1, d_beta, 1, 1.0, out, 1, tc, dw, st, nullptr))) return rc;
+  int herr = 0;
+  MSLR_CUDA_TRY(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MSLR_CUDA_TRY(cudaStreamSynchronize(st));
+  if (herr & kErrMmaWait)
+    return fail(MSLR_ERR_CUDA, "a tensor-core kernel's bounded wait for its MMAs timed out; "
+                               "the output is not valid");
+  return MSLR_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -771,8 +785,9 @@ int svst_batch_noalloc(int mrows, int ncols, int batch, const double* betas, con
     }
     scratch = g_noalloc_addr[dev];
   }
-  // No part of the scratch has to start at zero: every stage writes what the
-  // next one reads, so the previous call's contents are simply overwritten.
+  // The array keeps the previous call's contents.  Only the error word has to
+  // start at zero, and svst_batch clears it on the stream before the first
+  // kernel; every other stage writes what the next one reads.
   return svst_batch(mrows, ncols, batch, betas, in, out, scratch, (size_t)MSLR_NOALLOC_SCRATCH_BYTES,
                     MSLR_FORM_TUNED, st);
 }
@@ -807,7 +822,7 @@ int patch_nucnorm_all(Ctx* c, const cf* X, double* reg_out, cudaStream_t st) {
     const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
     const int nsplit = choose_split(g.Np, g.n, g.L);
     WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? k : 0].gram, g.Np, g.n, nsplit);
-    if ((rc = svst_gram(X + k * E, m, g.Np, w, nsplit, tc, st, &c->launches))) return rc;
+    if ((rc = svst_gram(X + k * E, m, g.Np, w, nsplit, tc, ctx_wait(c), st, &c->launches))) return rc;
     EigSegment seg;
     seg.n = g.n;
     seg.np = g.Np;
@@ -928,7 +943,7 @@ int svst_vjp_scale(Ctx* c, int s, const cf* z, const cf* xbar, double beta, cf* 
   w.aux = v.aux;
   w.rank = v.rank;
   w.part = v.part;
-  if ((rc = svst_gram(z, m, np, w, choose_split(np, n, g.L), false, st, &c->launches))) return rc;
+  if ((rc = svst_gram(z, m, np, w, choose_split(np, n, g.L), 0, ctx_wait(c), st, &c->launches))) return rc;
   EigSegment seg;
   seg.n = n;
   seg.np = np;
@@ -975,7 +990,9 @@ int tune_svst_splits(Ctx* c, cudaStream_t st) {
     for (int ns = cap; ns >= 1; ns = (ns > 1 && ns / 2 == 0) ? 1 : ns / 2) {
       WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? k : 0].gram, g.Np, g.n, ns);
       float ms = 0.f;
-      int rc = time_ms(st, 3, &ms, [&] { return svst_gram(c->d_ahy, m, 1, w, ns, c->tc_mode(), st, nullptr); });
+      int rc = time_ms(st, 3, &ms, [&] {
+        return svst_gram(c->d_ahy, m, 1, w, ns, c->tc_mode(), ctx_wait(c), st, nullptr);
+      });
       if (rc) return rc;
       if (ms < best) {
         best = ms;

@@ -20,7 +20,7 @@ module MSLRB200
 using CUDA
 
 export MSLRContext, sense_forward!, sense_adjoint!, dc_cost_grad!, patch_svst!,
-       pogm_run!, power_iter, mslr_lambdas, set_lambdas!, pogm_grad, mslr_sampling
+       pogm_run!, cost, sync!, power_iter, mslr_lambdas, set_lambdas!, pogm_grad, mslr_sampling
 
 const libmslr = get(ENV, "MSLR_LIB", joinpath(@__DIR__, "..", "libmslr.so"))
 
@@ -146,22 +146,64 @@ function patch_svst!(out::CuArray{ComplexF32}, ctx::MSLRContext, img::CuArray{Co
 end
 
 """
-    pogm_run!(ctx, X, niter, L; restart_cutoff=0.0, bsig=1.0) -> restarts
+    pogm_run!(ctx, X, niter, L; restart_cutoff=0.0, bsig=1.0, costs=false)
 
 `pogm_mod(X, ..., dc_cost_grad, L; mom=:pogm, restart=:gr, niter, g_prox)`
 with run_recon's closures, overwriting `X` `(Nx,Ny,Nz,Nt,Ns)`.  Returns the
 per-iteration restart flags (entry 1 is false, as the logger's first entry).
-Cost logging is not computed.
+With `costs=true` it returns `(dc_costs, reg_costs, restarts)`, the three
+vectors run_recon's logger collects and saves
+(scripts/reconstruct.jl:204-205, :228-230): the costs of X0 and of every
+iterate, FP64.
 """
 function pogm_run!(ctx::MSLRContext, X::CuArray{ComplexF32}, niter::Integer, L::Real;
-                   restart_cutoff::Real=0.0, bsig::Real=1.0)
+                   restart_cutoff::Real=0.0, bsig::Real=1.0, costs::Bool=false)
     flags = zeros(UInt8, niter + 1)
+    if costs
+        dc = zeros(Float64, niter + 1)
+        reg = zeros(Float64, niter + 1)
+        _check(ccall((:mslr_pogm_run_costs, libmslr), Cint,
+                     (Ptr{Cvoid}, CuPtr{ComplexF32}, Int32, Float64, Float64, Float64, Ptr{UInt8},
+                      Ptr{Float64}, Ptr{Float64}, Ptr{Cvoid}),
+                     ctx.h, X, Int32(niter), Float64(L), Float64(restart_cutoff), Float64(bsig),
+                     flags, dc, reg, _stream()), ctx.h)
+        return dc, reg, Bool.(flags)
+    end
     _check(ccall((:mslr_pogm_run, libmslr), Cint,
                  (Ptr{Cvoid}, CuPtr{ComplexF32}, Int32, Float64, Float64, Float64, Ptr{UInt8},
                   Ptr{Cvoid}),
                  ctx.h, X, Int32(niter), Float64(L), Float64(restart_cutoff), Float64(bsig),
                  flags, _stream()), ctx.h)
     return Bool.(flags)
+end
+
+"""
+    cost(ctx, X) -> (dc_cost, reg_cost)
+
+The two terms of run_recon's cost for `X` `(Nx,Ny,Nz,Nt,Ns)`
+(scripts/reconstruct.jl:176-194): ½‖A Σ_k X[..,k] − y‖² and
+Σ_k λ_k patch_nucnorm(img2patches(X[..,k])), FP64.
+"""
+function cost(ctx::MSLRContext, X::CuArray{ComplexF32})
+    dc = Ref{Float64}(0.0)
+    reg = Ref{Float64}(0.0)
+    _check(ccall((:mslr_cost, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, Int32, Ref{Float64}, Ref{Float64}, Ptr{Cvoid}),
+                 ctx.h, X, Int32(size(X, 5)), dc, reg, _stream()), ctx.h)
+    return dc[], reg[]
+end
+
+"""
+    sync!(ctx)
+
+Wait for the context's work on the task-local stream and raise any error its
+kernels recorded since the last check (a bounded wait that ran out, a
+non-finite restart sum) — the asynchronous calls (`dc_cost_grad!`,
+`patch_svst!`, the operators) leave those to the next synchronising call.
+"""
+function sync!(ctx::MSLRContext)
+    _check(ccall((:mslr_sync, libmslr), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), ctx.h, _stream()), ctx.h)
+    return ctx
 end
 
 """X0 of scripts/reconstruct.jl:209-214: X[..,1] = A'y, other scales 0."""

@@ -46,14 +46,7 @@ def run_recon(smaps, y, idx, patch_sizes, strides, niters: int, sigma1=None, for
         X = ctx.init_x0()
         dcs, regs = [], []
         if log_costs:
-            ctx.pogm_begin(X, niters, L, restart_cutoff, bsig)
-            for it in range(niters + 1):
-                if it:
-                    ctx.pogm_step(X)
-                dc, reg = ctx.cost(X)
-                dcs.append(dc)
-                regs.append(reg)
-            restarts = ctx.pogm_restarts()
+            restarts, dcs, regs = ctx.pogm_run_costs(X, niters, L, restart_cutoff, bsig)
         else:
             restarts = ctx.pogm_run(X, niters, L, restart_cutoff, bsig)
         torch.cuda.synchronize()

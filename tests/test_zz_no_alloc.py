@@ -7,7 +7,9 @@ may run on a fixed memory plan.  ``mslr_svst_batch_noalloc`` serves them by
 using a fixed 16 MiB device array inside the library as its scratch.  This
 test calls it through the C ABI twice in a row and compares each result with
 the workspace-taking ``mslr_svst_batch`` on the same input, within the
-tolerance the other SVST tests use.  It lives in its own file, collected
+tolerance the other SVST tests use, and with the FP64 oracle's SVST.  It
+also checks that a bounded wait cut short (``mslr_set_wait_limit``) makes
+the call fail instead of returning a partial result.  It lives in its own file, collected
 last, and passes both alone in a fresh process and after the other tests.
 """
 import ctypes as C
@@ -15,6 +17,8 @@ import os
 
 import numpy as np
 import pytest
+
+from oracle import mslr_oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -60,6 +64,24 @@ def test_noalloc_matches_workspace_entry_point():
         a, b = out_na.cpu().numpy(), out_ws.cpu().numpy()
         assert np.all(a[3] == 0)
         assert _rel(a, b) < 2e-5, (call, _rel(a, b))
+        # and against the FP64 oracle (thin SVD, singular values soft-thresholded)
+        for k in (0, batch - 1):
+            ref = O.svst(X[k].T.astype(np.complex128), betas[k]).T
+            assert _rel(a[k], ref) < 1e-4, (call, k, _rel(a[k], ref))
+
+    # a bounded wait that runs out is reported, not returned as a result: the
+    # call fails with MSLR_ERR_CUDA, and the next call is right again
+    lib.mslr_set_wait_limit.argtypes = [P, C.c_int64]
+    assert lib.mslr_set_wait_limit(None, 0) == 0
+    try:
+        rc = lib.mslr_svst_batch_noalloc(m, n, batch, betas, x_d.data_ptr(), out_na.data_ptr(), stream)
+        assert rc == 2
+        assert b"timed out" in lib.mslr_last_error(None)
+    finally:
+        assert lib.mslr_set_wait_limit(None, 1 << 22) == 0
+    rc = lib.mslr_svst_batch_noalloc(m, n, batch, betas, x_d.data_ptr(), out_na.data_ptr(), stream)
+    assert rc == 0, lib.mslr_last_error(None)
+    assert _rel(out_na.cpu().numpy(), out_ws.cpu().numpy()) < 2e-5
 
     # a batch larger than the fixed scratch is refused with a clear message
     bet = (D * 64)(*([1.0] * 64))
