@@ -36,6 +36,7 @@ Every function cites the reference file:line it restates.
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass
 from typing import Callable, List, Sequence
 
@@ -483,6 +484,245 @@ def run_recon_arrays(prob: ReconProblem, niters: int, dtype=np.complex128, log_c
                      g_prox=g_prox, fun=logger, iter_callback=iter_callback,
                      restart_cutoff=restart_cutoff, bsig=bsig)
     return Xf, restarts, dcs, regs
+
+
+# ---------------------------------------------------------------------------
+# Full-size runs (the benchmark's 90×90×60 workloads).  The same arithmetic as
+# run_recon_arrays — per-frame SENSE of src/sense_gpu.jl:71-101, per-patch
+# gesdd SVST of src/recon.jl:183-211 with the ascending-ip recombine of
+# :96-126, and pogm_mod's aliased recurrence (src/mirt_mod.jl:144-176 with
+# run_recon's in-place g_prox, scripts/reconstruct.jl:196-202) — organised
+# for host memory and cores: frames, patches and update chunks are spread
+# over a thread pool (as the reference's @threads over patches), patches are
+# extracted and recombined one at a time instead of as a whole patch stack,
+# and the recurrence is written out with the aliasing resolved (xold is
+# zold, so the β·α/ζold·(xold − zold) term is zero, Fgrad = fgrad and
+# ynew = unew) and evaluated in place.  tests/test_oracle.py pins it to
+# run_recon_arrays.
+# ---------------------------------------------------------------------------
+def _pool_map(pool, fn, items, window: int = 256):
+    """Ordered map over ``items`` with at most ``window`` tasks in flight."""
+    items = list(items)
+    for i0 in range(0, len(items), window):
+        yield from pool.map(fn, items[i0:i0 + window])
+
+
+class _ShiftedSense:
+    """sense_forward_frame / sense_adjoint_frame with the centring shifts
+    moved onto the coil maps and the sample indices.  For even image sizes
+    fftshift and ifftshift are the same permutation p of the grid, an
+    involution, so fftshift(fft(ifftshift(S·x)))[idx] = fft(pS · px)[p(idx)]
+    and Σ_c conj(S_c)·fftshift(Y_c) = fftshift(Σ_c conj(pS_c)·Y_c): the same
+    products and sums on permuted arrays (equal to the plain functions up to
+    the FFT library's FP64 rounding, which depends on memory layout), with
+    the shifted maps made once instead of every frame's coil images shifted
+    twice.  Odd sizes use the plain functions."""
+
+    def __init__(self, smaps: np.ndarray):
+        self.smaps = smaps
+        Nc, Nz, Ny, Nx = smaps.shape
+        self.even = Nz % 2 == 0 and Ny % 2 == 0 and Nx % 2 == 0
+        self.n = Nx * Ny * Nz
+        self.scale = 1.0 / math.sqrt(self.n)
+        if self.even:
+            self.ps = sfft.ifftshift(smaps, axes=SPATIAL_AXES)
+            self.pc = np.conj(self.ps)
+            self.perm = sfft.ifftshift(np.arange(self.n).reshape(Nz, Ny, Nx)).reshape(-1)
+
+    def forward(self, x: np.ndarray, idx: np.ndarray) -> np.ndarray:
+        if not self.even:
+            return sense_forward_frame(x, self.smaps, idx, 1)
+        Nc = self.ps.shape[0]
+        k = sfft.fftn(self.ps * sfft.ifftshift(x)[None], axes=SPATIAL_AXES, workers=1, overwrite_x=True)
+        return k.reshape(Nc, -1)[:, self.perm[idx]] * self.scale
+
+    def adjoint(self, y: np.ndarray, idx: np.ndarray) -> np.ndarray:
+        if not self.even:
+            return sense_adjoint_frame(y, self.smaps, idx, 1)
+        Nc, Nz, Ny, Nx = self.ps.shape
+        full = np.zeros((Nc, self.n), dtype=np.result_type(y.dtype, self.ps.dtype))
+        full[:, self.perm[idx]] = y
+        xc = sfft.ifftn(full.reshape(Nc, Nz, Ny, Nx), axes=SPATIAL_AXES, workers=1, overwrite_x=True)
+        xc *= self.n
+        xc *= self.scale
+        return sfft.fftshift(np.sum(self.pc * xc, axis=0))
+
+
+def dc_grad_frames(X: np.ndarray, smaps: np.ndarray, y: np.ndarray, idx: np.ndarray, pool,
+                   out: np.ndarray | None = None, sense: _ShiftedSense | None = None) -> np.ndarray:
+    """dc_cost_grad before the repeat (scripts/reconstruct.jl:180-183),
+    g[t] = A_t'(A_t Σ_k X[k, t] − y[t]), frames in parallel."""
+    Ns, Nt = X.shape[:2]
+    g = np.empty(X.shape[1:], dtype=X.dtype) if out is None else out
+    sense = sense or _ShiftedSense(smaps)
+
+    def frame(t):
+        xs = X[0, t].copy()
+        for k in range(1, Ns):
+            xs += X[k, t]
+        r = sense.forward(xs, idx[t]) - y[t]
+        g[t] = sense.adjoint(r, idx[t])
+        return t
+
+    for _ in _pool_map(pool, frame, range(Nt)):
+        pass
+    return g
+
+
+def adjoint_frames(y: np.ndarray, smaps: np.ndarray, idx: np.ndarray, pool,
+                   sense: _ShiftedSense | None = None) -> np.ndarray:
+    """A'y frame by frame in parallel (X0 of scripts/reconstruct.jl:209-214)."""
+    Nt = y.shape[0]
+    Nc, Nz, Ny, Nx = smaps.shape
+    out = np.empty((Nt, Nz, Ny, Nx), dtype=np.result_type(y.dtype, smaps.dtype))
+    sense = sense or _ShiftedSense(smaps)
+
+    def frame(t):
+        out[t] = sense.adjoint(y[t], idx[t])
+        return t
+
+    for _ in _pool_map(pool, frame, range(Nt)):
+        pass
+    return out
+
+
+def patch_svst_inplace(img: np.ndarray, beta: float, patch_size, stride_size, pool,
+                       blas_threads: int = 1) -> np.ndarray:
+    """patch_svst (src/recon.jl:251-256) into ``img`` itself, one patch at a
+    time: SVST of every patch of the input, sums in ascending ip, FP32
+    coverage count clamped to 1, component-wise division.  A single-patch
+    scale runs its one SVD with ``blas_threads`` BLAS threads."""
+    Nt, Nz, Ny, Nx = img.shape
+    g = patch_geometry((Nx, Ny, Nz), patch_size, stride_size)
+    psx, psy, psz = g.ps
+
+    def block(ip):
+        sx, sy, sz = g.patch_start(ip)
+        return (slice(None), slice(sz, sz + psz), slice(sy, sy + psy), slice(sx, sx + psx))
+
+    def one(ip):
+        P = img[block(ip)].reshape(Nt, g.p)
+        return svst(P.T.copy(), beta).T.reshape(Nt, psz, psy, psx)
+
+    out = np.zeros_like(img)
+    if g.Np == 1:
+        from threadpoolctl import threadpool_limits
+        with threadpool_limits(blas_threads, "blas"):
+            res = one(0)
+        out[block(0)] += res
+        del res
+    else:
+        for ip, res in zip(range(g.Np), _pool_map(pool, one, range(g.Np))):
+            out[block(ip)] += res
+    cnt = coverage_count((Nx, Ny, Nz), patch_size, stride_size)
+    c = np.maximum(cnt, np.float32(1)).astype(img.real.dtype)
+    out.real /= c[None]
+    out.imag /= c[None]
+    img[...] = out
+    return img
+
+
+def run_recon_large(prob: ReconProblem, niters: int, iter_callback=None, threads: int | None = None,
+                    restart_cutoff: float = 0.0, bsig: float = 1.0, chunk: int = 1 << 20,
+                    log: Callable | None = None):
+    """run_recon_arrays in FP64 for full-size problems.  Returns (X, restarts);
+    ``iter_callback(it, X, is_restart)`` sees X after every iteration (X is
+    overwritten by the next one); ``log(phase, seconds)`` receives the time of
+    every phase."""
+    import time
+    from concurrent.futures import ThreadPoolExecutor
+    threads = threads or os.cpu_count() or 1
+    clock = [time.perf_counter()]
+
+    def lap(phase):
+        if log is not None:
+            t = time.perf_counter()
+            log(phase, t - clock[0])
+            clock[0] = t
+
+    Nx, Ny, Nz = prob.N
+    Nt, Ns = prob.Nt, prob.Ns
+    dtype = np.complex128
+    smaps = prob.smaps.astype(dtype)
+    y = prob.y.astype(dtype)
+    idx = prob.idx
+    lam = prob.lambdas()
+    L = prob.lipschitz()
+    restarts = [False]
+    sense = _ShiftedSense(smaps)
+    with ThreadPoolExecutor(threads) as pool:
+        x = np.zeros((Ns, Nt, Nz, Ny, Nx), dtype=dtype)
+        x[0] = adjoint_frames(y, smaps, idx, pool, sense)
+        lap("x0")
+        uold = x.copy()                          # u_0 = y_0 = x_0
+        g = np.empty((Nt, Nz, Ny, Nx), dtype=dtype)
+        gold = np.zeros_like(g) if bsig != 1.0 else None
+        u = np.empty_like(x)
+        told, sig = 1.0, 1.0
+        E = g.size
+        xf, uf, of, gf = x.reshape(Ns, E), u.reshape(Ns, E), uold.reshape(Ns, E), g.reshape(E)
+        for it in range(1, niters + 1):
+            alpha = 1.0 / L
+            dc_grad_frames(x, smaps, y, idx, pool, out=g, sense=sense)
+            lap("dc_grad")
+            tnew = 0.5 * (1 + math.sqrt(1 + (8 if it == niters else 4) * told ** 2))
+            beta = (told - 1) / tnew
+            gamma = sig * told / tnew
+
+            # u = x − α g;  restart sums over u − uold;  z = u + β(u − uold) + γ(u − x) into x;
+            # chunks in parallel, their partial sums added in chunk order
+            def update(e0, xf=xf, uf=uf, of=of):
+                sl = slice(e0, min(E, e0 + chunk))
+                gs = gf[sl]
+                part = [0.0, 0.0, float(np.vdot(gs, gs).real), 0.0]
+                if gold is not None:
+                    part[3] = float(np.sum(np.real(gs * gold.reshape(E)[sl]), dtype=np.float64))
+                for k in range(Ns):
+                    uk = xf[k, sl] - alpha * gs
+                    du = uk - of[k, sl]
+                    part[0] += float(np.sum(np.real(-gs * du), dtype=np.float64))
+                    part[1] += float(np.vdot(du, du).real)
+                    xf[k, sl] = uk + beta * du + gamma * (uk - xf[k, sl])
+                    uf[k, sl] = uk
+                return part
+
+            dot, n_du, n_g, gg = 0.0, 0.0, 0.0, 0.0
+            for p0, p1, p2, p3 in _pool_map(pool, update, range(0, E, chunk)):
+                dot, n_du, n_g, gg = dot + p0, n_du + p1, n_g + p2, gg + p3
+            lap("update")
+            zeta = alpha * (1 + beta + gamma)
+            for k in range(Ns):
+                patch_svst_inplace(x[k], zeta * lam[k], prob.patch_sizes[k], prob.strides[k], pool,
+                                   blas_threads=threads)
+                lap(f"svst_{k}")
+            # _gr_restart with Fgrad = the Ns-fold repeat of g, ynew − yold = u − uold
+            rhs = restart_cutoff * math.sqrt(Ns * n_g) * math.sqrt(n_du)
+            is_restart = dot <= rhs
+            if is_restart:
+                tnew, sig = 1.0, 1.0
+            elif gold is not None and Ns * gg < 0:
+                sig = bsig * sig
+            if gold is not None:
+                gold[...] = g
+            restarts.append(bool(is_restart))
+            u, uold = uold, u
+            uf, of = of, uf
+            told = tnew
+            if iter_callback is not None:
+                iter_callback(it, x, is_restart)
+    return x, restarts
+
+
+def rel_err_chunked(a: np.ndarray, b: np.ndarray, chunk: int = 1 << 22) -> float:
+    """:func:`rel_err` of two large arrays without full-size FP64 copies."""
+    af, bf = a.reshape(-1), b.reshape(-1)
+    num = den = 0.0
+    for e0 in range(0, af.size, chunk):
+        d = af[e0:e0 + chunk].astype(np.complex128) - bf[e0:e0 + chunk]
+        bb = bf[e0:e0 + chunk].astype(np.complex128)
+        num += float(np.vdot(d, d).real)
+        den += float(np.vdot(bb, bb).real)
+    return math.sqrt(num) / (math.sqrt(den) if den > 0 else 1.0)
 
 
 def rel_err(a: np.ndarray, b: np.ndarray) -> float:

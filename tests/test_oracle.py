@@ -208,3 +208,38 @@ def test_golden_fixtures_reproduce():
     ref = np.load(path)
     for k in ref.files:
         np.testing.assert_allclose(fresh[k], ref[k], rtol=1e-9, atol=1e-9, err_msg=k)
+
+
+@pytest.mark.parametrize("case", ["small", "overlap", "bsig"])
+def test_large_runner_is_run_recon_arrays(synth, case):
+    """The full-size runner (threads over frames, patches and update chunks,
+    shifts moved onto the coil maps, in-place recurrence with the aliasing
+    resolved) gives run_recon_arrays' iterates and restart flags: the runner
+    the full-size parity tests use is the same oracle."""
+    import dataclasses
+    kw = {}
+    if case == "small":
+        cfg = dataclasses.replace(synth.CONFIGS["small"], Nt=16)
+    elif case == "overlap":   # a global patch, half-overlapping and clamped edge patches
+        cfg = dataclasses.replace(synth.CONFIGS["small"], N=(14, 12, 10), Nt=10, Nc=4,
+                                  patch_sizes=[[14, 12, 10], [4, 4, 4], [3, 3, 3]],
+                                  strides=[[14, 12, 10], [2, 2, 2], [3, 3, 3]])
+    else:                     # the σ decrease of pogm_mod (bsig < 1), no restarts
+        cfg = dataclasses.replace(synth.CONFIGS["small"], N=(12, 10, 8), Nt=12, Nc=3,
+                                  patch_sizes=[[12, 10, 8], [4, 5, 4]], strides=[[12, 10, 8], [4, 5, 4]])
+        kw = {"bsig": 0.5, "restart_cutoff": -0.3}
+    pb = synth.make_problem(cfg)
+    prob = O.ReconProblem(smaps=pb["smaps"].astype(np.complex128), idx=pb["idx"],
+                          y=pb["y"].astype(np.complex128), patch_sizes=pb["patch_sizes"],
+                          strides=pb["strides"], sigma1=0.7, workers=1)
+    niter = 8
+    ref = []
+    _, r_ref, _, _ = O.run_recon_arrays(prob, niter, iter_callback=lambda it, xk, r: ref.append(xk.copy()),
+                                        **kw)
+    got = []
+    _, r_got = O.run_recon_large(prob, niter, iter_callback=lambda it, xk, r: got.append(xk.copy()),
+                                 threads=3, chunk=1000, **kw)
+    assert r_got == r_ref
+    for a, b in zip(got, ref):
+        assert O.rel_err(a, b) < 1e-12
+        assert O.rel_err_chunked(a, b, chunk=777) == pytest.approx(O.rel_err(a, b), rel=1e-9, abs=1e-300)
