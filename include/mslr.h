@@ -159,11 +159,16 @@ int mslr_normal_op(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g,
 
 /* Profiling hook (no counterpart in the reference): runs mslr_normal_op with
  * subtract_data = 1 once, recording CUDA events on `stream` around every
- * kernel, and returns the average device time per launch of the three
- * kernels of a chunk — kernel_ms[0] forward z pass, [1] plane (x, y, mask)
- * pass, [2] adjoint z pass with the coil combine — and the launches of each.
- * Synchronises `stream`.  MSLR_ERR_UNSUPPORTED unless the tuned form runs the
- * shape-specialised SENSE kernels for this image shape. */
+ * kernel of every chunk, and returns in kernel_ms[0..3] the average device
+ * time per launch of the chunk's kernels and in launches_per_kernel[0..3]
+ * their launch counts.  Four-pass form (the default): [0] forward plane pass
+ * (coil maps × summed image, DFT_y, DFT_x), [1] z pass with the k-space mask,
+ * [2] inverse plane pass with × conj(coil map), [3] coil combine.  Three-kernel
+ * form (MSLR_SENSE_PATH=3, or the tensor-core plane pass): [0] forward z pass,
+ * [1] plane pass, [2] adjoint z pass with the coil combine, [3] zero.  Both
+ * arrays must hold 4 entries.  Synchronises `stream`.  MSLR_ERR_UNSUPPORTED
+ * unless the tuned form runs the shape-specialised SENSE kernels for this
+ * image shape. */
 int mslr_normal_op_profile(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g, void* stream,
                            double* kernel_ms, int64_t* launches_per_kernel);
 

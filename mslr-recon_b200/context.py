@@ -184,8 +184,11 @@ class MSLRContext:
         self._chk(lib.mslr_set_graph(self._h, 1 if enable else 0))
 
     def normal_profile(self, X: torch.Tensor, out=None, stream=None):
-        """One normal operator with events around every kernel: returns
-        ({"zfwd": ms, "xy": ms, "zadj": ms} average per launch, launches of each)."""
+        """One normal operator with events around every kernel of every chunk:
+        returns ({kernel: average ms per launch}, launches of each).  Kernels of
+        the four-pass form: "pfwd" (forward plane pass), "zmask" (z pass with
+        the mask), "padj" (inverse plane pass), "csum" (coil combine); of the
+        three-kernel form: "zfwd", "xy", "zadj"."""
         import ctypes as C
         if X.dim() == 4:
             X = X.unsqueeze(0)
@@ -193,10 +196,12 @@ class MSLRContext:
         _dev_c64(X, (ns,) + self.img_shape, "X")
         g = out if out is not None else torch.empty(self.img_shape, dtype=torch.complex64,
                                                     device=X.device)
-        ms = (C.c_double * 3)()
-        n = (C.c_int64 * 3)()
+        ms = (C.c_double * 4)()
+        n = (C.c_int64 * 4)()
         self._chk(lib.mslr_normal_op_profile(self._h, X.data_ptr(), ns, g.data_ptr(),
                                              _stream_ptr(stream), ms, n))
+        if n[3] > 0:
+            return {"pfwd": ms[0], "zmask": ms[1], "padj": ms[2], "csum": ms[3]}, int(n[0])
         return {"zfwd": ms[0], "xy": ms[1], "zadj": ms[2]}, int(n[0])
 
     def patch_svst(self, scale: int, beta: float, img: torch.Tensor, out=None, stream=None):

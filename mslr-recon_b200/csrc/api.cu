@@ -69,6 +69,7 @@ static void free_ctx(mslr_ctx* c) {
   if (c->d_ckpt) cudaFree(c->d_ckpt);
   if (c->d_gbuf) cudaFree(c->d_gbuf);
   if (c->d_vjpw) cudaFree(c->d_vjpw);
+  if (c->d_xsum) cudaFree(c->d_xsum);
   delete c;
 }
 
@@ -320,22 +321,25 @@ int mslr_normal_op_profile(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g,
                            reinterpret_cast<cf*>(g), true, st);
   ctx->prof_on = false;
   if (rc) return ctx_fail(ctx, rc);
-  if (ctx->prof_n % 4) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "profiling events out of step"));
+  const int nk = ctx->prof_kernels, per = nk + 1;
+  if (ctx->prof_n == 0 || ctx->prof_n % per)
+    return ctx_fail(ctx, fail(MSLR_ERR_CUDA, "profiling events out of step"));
   cudaError_t e = cudaEventSynchronize(ctx->prof_ev[ctx->prof_n - 1]);
   if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
-  double tot[3] = {0.0, 0.0, 0.0};
-  const int chunks = ctx->prof_n / 4;
+  double tot[4] = {0.0, 0.0, 0.0, 0.0};
+  const int chunks = ctx->prof_n / per;
   for (int q = 0; q < chunks; ++q)
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0; k < nk; ++k) {
       float ms = 0.f;
-      e = cudaEventElapsedTime(&ms, ctx->prof_ev[4 * q + k], ctx->prof_ev[4 * q + k + 1]);
+      e = cudaEventElapsedTime(&ms, ctx->prof_ev[per * q + k], ctx->prof_ev[per * q + k + 1]);
       if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
       tot[k] += ms;
     }
-  for (int k = 0; k < 3; ++k) {
-    kernel_ms[k] = chunks ? tot[k] / chunks : 0.0;
-    launches_per_kernel[k] = chunks;
+  for (int k = 0; k < 4; ++k) {
+    kernel_ms[k] = (k < nk && chunks) ? tot[k] / chunks : 0.0;
+    launches_per_kernel[k] = k < nk ? chunks : 0;
   }
+  CTX_RET(ctx, take_error(ctx, st));
   return MSLR_OK;
 }
 

@@ -91,6 +91,13 @@ struct Ctx {
   int spec_ch = 6;        // coils per group of the specialised normal operator (autotuned)
   int spec_fr = 2;        // frames per chunk (autotuned)
   int spec_zfwd_ctas = 0; // resident CTAs of the specialised forward z kernel
+  // four-pass form of the specialised normal operator (default; MSLR_SENSE_PATH=3
+  // selects the three-kernel form): resident CTAs of its kernels, and the
+  // summed image Σ_k X_k of all frames that its forward plane pass reads
+  bool spec_four = true;
+  int spec_pfwd_ctas = 0, spec_zmask_ctas = 0, spec_padj_ctas = 0;
+  bool spec_zmask1 = false;   // z-mask kernel variant with one CTA per SM
+  cf* d_xsum = nullptr;   // (Nt, nvox)
   bool xy_tc = false;     // tensor-core plane pass (DFT products on tcgen05)
   uint32_t* d_dft = nullptr;   // its split-BF16 DFT matrix tiles
   // graph-captured POGM step (tuned form): captured on a private stream the
@@ -110,6 +117,7 @@ struct Ctx {
   bool prof_on = false;
   std::vector<cudaEvent_t> prof_ev;
   int prof_n = 0;   // events recorded in the current profiled call
+  int prof_kernels = 3;   // kernels per chunk of the profiled call (events per chunk: + 1)
 
   // POGM
   cf* d_U = nullptr;   // (Ns, Nt, nvox)

@@ -80,6 +80,11 @@ struct Shape {
   static constexpr size_t smem_zadj = sizeof(cf) * (2 * (size_t)S + ev(NZ)) + sizeof(uint64_t);
   static constexpr size_t smem_xy =
       sizeof(cf) * (2 * (size_t)PL + ev(NX) + ev(NY)) + MW * sizeof(uint32_t) + sizeof(uint64_t);
+  // four-pass form
+  static constexpr size_t smem_pfwd = sizeof(cf) * (3 * (size_t)PL + ev(NX) + ev(NY)) + sizeof(uint64_t);
+  static constexpr size_t smem_zmask =
+      sizeof(cf) * (2 * (size_t)S + ev(NZ)) + 4 * NZ * sizeof(uint32_t) + 2 * sizeof(uint64_t);
+  static constexpr size_t smem_padj = sizeof(cf) * (2 * (size_t)PL + ev(NX) + ev(NY)) + sizeof(uint64_t);
 };
 
 // xs[z][x] · S'_c[z][x], both in shared memory (line = x, element = z)
@@ -370,6 +375,377 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, 2)
   cluster.sync();
 }
 
+// ===========================================================================
+// Four-pass form of the normal operator (the default).  Per chunk of frames
+// and group of coils, with T[f][cc][z][y][x] the chunk's per-coil k-space:
+//   k_pfwd   unit (cc, z, f): S'_c ⊙ x̄ on plane z → DFT_y → DFT_x → T
+//            (x̄ = Σ_k X_k, summed once per operator by k_xsum)
+//   k_zmask  unit (cc, f, y): the z slab of T → DFT_z → mask → bDFT_z → T,
+//            in place, slabs in and out by bulk copies
+//   k_padj   unit (cc, z, f): plane of T → bDFT_y → bDFT_x → × conj(S'_c) → T
+//   k_csum   g (=, −A'y, or +=) scale · Σ_cc T[f][cc], coils summed in order
+// The plane passes take their planes by TMA (the next unit's while the current
+// one runs its row passes); every unit is one plane or slab, so the launches
+// fill all SMs evenly and no CTA waits on another.
+// ===========================================================================
+
+// x̄[i] = Σ_k X[k][i] over ns scales (in order), n elements, pairs per thread
+__global__ void k_xsum(const cf* __restrict__ X, int ns, int64_t sstride, cf* __restrict__ out,
+                       int64_t n) {
+  const int64_t step = (int64_t)gridDim.x * blockDim.x;
+  const bool vec = ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(out)) & 15) == 0 &&
+                   (sstride % 2) == 0 && (n % 2) == 0;
+  if (vec) {
+    const float4* x4 = reinterpret_cast<const float4*>(X);
+    float4* o4 = reinterpret_cast<float4*>(out);
+    const int64_t n2 = n / 2, s2 = sstride / 2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += step) {
+      float4 v = x4[i];
+      for (int k = 1; k < ns; ++k) {
+        const float4 w = x4[i + k * s2];
+        v.x += w.x;
+        v.y += w.y;
+        v.z += w.z;
+        v.w += w.w;
+      }
+      o4[i] = v;
+    }
+    return;
+  }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += step) {
+    cf v = X[i];
+    for (int k = 1; k < ns; ++k) v = cadd(v, X[i + k * sstride]);
+    out[i] = v;
+  }
+}
+
+// a[i] · b[i], both in shared memory (line l, element e at l·SL + e·SE)
+template <int SL, int SE>
+struct LdMul {
+  const cf* a;
+  const cf* b;
+  __device__ __forceinline__ cf operator()(int l, int e) const {
+    return cmul(a[l * SL + e * SE], b[l * SL + e * SE]);
+  }
+};
+// dst[i] = conj(s[i]) · v, row layout (line = row, element = x); s in global memory
+template <int NX>
+struct StMulC {
+  cf* dst;
+  const cf* s;
+  __device__ __forceinline__ void operator()(int l, int e, cf v) const {
+    const int i = l * NX + e;
+    dst[i] = cmulc(__ldg(s + i), v);
+  }
+};
+// k-space mask of one z slab (line = kx, element = kz): row kz's bits start at
+// bit (kz·PL + y·NX) & 31 of the four words w[4·kz ..]
+template <int NX, int PL>
+struct MaskZ {
+  const uint32_t* w;
+  int ybit;   // y·NX
+  __device__ __forceinline__ cf operator()(int l, int e, cf v) const {
+    const int b = ((e * PL + ybit) & 31) + l;
+    return ((w[4 * e + (b >> 5)] >> (b & 31)) & 1u) ? v : make_float2(0.f, 0.f);
+  }
+};
+
+// Pass groups of the plane kernels, out of line (each keeps its own index
+// arithmetic, within the 128-register budget of 16 warps).
+template <class Sh>
+__device__ __noinline__ void pf_cols(const cf* xs, const cf* sc, cf* W, const cf* twy, int l0) {
+  using AY = typename Sh::AY;
+  using Cols = SmC<1, Sh::NX>;
+  spec::wpass<Sh::NY, AY::R0, 1, false, AY::LPW, false>(l0, Sh::NX, twy, LdMul<1, Sh::NX>{xs, sc},
+                                                        Cols{W});
+  spec::wpass<Sh::NY, AY::R1, AY::R0, false, AY::LPW, true>(l0, Sh::NX, twy, Cols{W}, Cols{W});
+}
+template <class Sh>
+__device__ __noinline__ void pf_rows(cf* W, const cf* twx, int l0, cf* dst) {
+  using AX = typename Sh::AX;
+  using Rows = SmC<Sh::NX, 1>;
+  spec::wpass<Sh::NX, AX::R0, 1, false, AX::LPW, true>(l0, Sh::NY, twx, Rows{W}, Rows{W});
+  spec::wpass<Sh::NX, AX::R1, AX::R0, false, AX::LPW, false>(l0, Sh::NY, twx, Rows{W}, Rows{dst});
+}
+template <class Sh>
+__device__ __noinline__ void pa_cols(const cf* P, cf* W, const cf* twy, int l0) {
+  using AY = typename Sh::AY;
+  using Cols = SmC<1, Sh::NX>;
+  spec::wpass<Sh::NY, AY::R1, 1, true, AY::LPW, false>(l0, Sh::NX, twy, Cols{const_cast<cf*>(P)},
+                                                       Cols{W});
+  spec::wpass<Sh::NY, AY::R0, AY::R1, true, AY::LPW, true>(l0, Sh::NX, twy, Cols{W}, Cols{W});
+}
+template <class Sh>
+__device__ __noinline__ void pa_rows(cf* W, const cf* twx, int l0, cf* dst, const cf* sc) {
+  using AX = typename Sh::AX;
+  using Rows = SmC<Sh::NX, 1>;
+  spec::wpass<Sh::NX, AX::R1, 1, true, AX::LPW, true>(l0, Sh::NY, twx, Rows{W}, Rows{W});
+  spec::wpass<Sh::NX, AX::R0, AX::R1, true, AX::LPW, false>(l0, Sh::NY, twx, Rows{W},
+                                                            StMulC<Sh::NX>{dst, sc});
+}
+
+// Forward plane pass of one coil group, persistent over units u = (cc
+// fastest, then z, then frame f of the chunk): the summed image plane and the
+// coil-map plane arrive by TMA; DFT_y over the columns of their product, then
+// DFT_x over the rows, written to T[f][cc][z].
+template <class Sh>
+__global__ void __launch_bounds__(Sh::XYW * 32, 1)
+    k_pfwd(const cf* __restrict__ xsum, int t0, int nf, int cc0, int ch, const cf* __restrict__ smod,
+           cf* __restrict__ T, const cf* __restrict__ twx_g, const cf* __restrict__ twy_g,
+           int* __restrict__ err) {
+  using AX = typename Sh::AX;
+  using AY = typename Sh::AY;
+  constexpr int NX = Sh::NX, NY = Sh::NY, NZ = Sh::NZ, PL = Sh::PL;
+  constexpr int64_t NVOX = Sh::NVOX;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  cf* XS = reinterpret_cast<cf*>(smraw);
+  cf* SB = XS + PL;
+  cf* W = SB + PL;
+  cf* twx = W + PL;
+  cf* twy = twx + Sh::ev(NX);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(twy + Sh::ev(NY));
+  const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int units = ch * NZ * nf;
+  auto issue = [&](int u) {
+    const int cc = u % ch, r = u / ch, z = r % NZ, f = r / NZ;
+    spec::mbar_expect_tx(bar, 2u * PL * (unsigned)sizeof(cf));
+    spec::bulk_g2s(XS, xsum + (int64_t)(t0 + f) * NVOX + (int64_t)z * PL, PL * (unsigned)sizeof(cf), bar);
+    spec::bulk_g2s(SB, smod + (int64_t)(cc0 + cc) * NVOX + (int64_t)z * PL, PL * (unsigned)sizeof(cf), bar);
+  };
+  if (tid == 0) {
+    spec::mbar_init(bar, 1);
+    spec::mbar_fence_init();
+  }
+  for (int i = tid; i < NX; i += blockDim.x) twx[i] = twx_g[i];
+  for (int i = tid; i < NY; i += blockDim.x) twy[i] = twy_g[i];
+  __syncthreads();
+  int u = blockIdx.x;
+  if (tid == 0 && u < units) issue(u);
+  unsigned par = 0;
+  bool bad = false;
+  for (; u < units; u += gridDim.x) {
+    if (!bad && !spec::mbar_wait(bar, par)) bad = true;
+    par ^= 1u;
+    if (!bad) {
+#pragma unroll 1
+      for (int g = warp; g * AY::LPW < NX; g += nw) pf_cols<Sh>(XS, SB, W, twy, g * AY::LPW);
+    }
+    __syncthreads();   // columns done: XS, SB free
+    const int nxt = u + (int)gridDim.x;
+    if (tid == 0 && nxt < units) {
+      spec::fence_proxy_async();
+      issue(nxt);
+    }
+    if (!bad) {
+      const int cc = u % ch, r = u / ch, z = r % NZ, f = r / NZ;
+      cf* dst = T + ((int64_t)f * ch + cc) * NVOX + (int64_t)z * PL;
+#pragma unroll 1
+      for (int g = warp; g * AX::LPW < NY; g += nw) pf_rows<Sh>(W, twx, g * AX::LPW, dst);
+    }
+    __syncthreads();   // rows done: W free
+  }
+  if (__syncthreads_or(bad) && tid == 0) atomicOr(err, kErrWait);
+}
+
+// z pass with the k-space mask, in place on T, persistent over slabs u = (cc
+// fastest, then frame, then y): each slab (NZ rows of NX) comes in by bulk
+// copies into one of two buffers, runs DFT_z, the mask and bDFT_z (the last
+// forward and first inverse radix passes fused around the mask), and goes back
+// by bulk copies; the other buffer's slab is in flight meanwhile.  MINB: CTAs
+// per SM the register budget is set for.
+template <class Sh, int MINB>
+__global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
+    k_zmask(cf* __restrict__ T, const uint32_t* __restrict__ mask, int nwords, int t0, int nf, int ch,
+            const cf* __restrict__ twz_g, int* __restrict__ err) {
+  using AZ = typename Sh::AZ;
+  constexpr int NX = Sh::NX, NY = Sh::NY, NZ = Sh::NZ, S = Sh::S, PL = Sh::PL;
+  constexpr int64_t NVOX = Sh::NVOX;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  cf* SL = reinterpret_cast<cf*>(smraw);          // two slab buffers
+  cf* tw = SL + 2 * S;
+  uint32_t* MB = reinterpret_cast<uint32_t*>(tw + Sh::ev(NZ));   // 4 words per kz
+  uint64_t* bar = reinterpret_cast<uint64_t*>(MB + 4 * NZ);
+  const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5, lane = tid & 31;
+  const int units = ch * nf * NY;
+  auto slab = [&](int u) {
+    const int cc = u % ch, r = u / ch, f = r % nf, y = r / nf;
+    return T + ((int64_t)f * ch + cc) * NVOX + (int64_t)y * NX;
+  };
+  if (tid == 0) {
+    spec::mbar_init(&bar[0], 1);
+    spec::mbar_init(&bar[1], 1);
+    spec::mbar_fence_init();
+  }
+  for (int i = tid; i < NZ; i += blockDim.x) tw[i] = twz_g[i];
+  __syncthreads();
+  if (warp == 0) {
+    for (int q = 0; q < 2; ++q) {
+      const int u = blockIdx.x + q * (int)gridDim.x;
+      if (u < units) rows_g2s(SL + q * S, slab(u), NZ, NX, PL, &bar[q]);
+    }
+  }
+  bool bad = false;
+  int k = 0;
+  for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
+    const int b = k & 1;
+    const int r = u / ch, f = r % nf, y = r / nf;
+    {   // mask words of the slab: row kz spans bits [kz·PL + y·NX, + NX) of frame t0 + f
+      const uint32_t* mrow = mask + (int64_t)(t0 + f) * nwords;
+      for (int i = tid; i < 4 * NZ; i += blockDim.x) {
+        const int kz = i >> 2;
+        const int w = (int)(((int64_t)kz * PL + (int64_t)y * NX) >> 5) + (i & 3);
+        MB[i] = (w < nwords) ? __ldg(mrow + w) : 0u;
+      }
+    }
+    __syncthreads();   // mask words visible
+    if (!bad && !spec::mbar_wait(&bar[b], (unsigned)((k >> 1) & 1))) bad = true;
+    cf* P = SL + b * S;
+    if (!bad) {
+      const cf* twc = opaque(tw);
+      using Cols = SmC<1, NX>;   // line = x, element = z
+      const MaskZ<NX, PL> msk{MB, y * NX};
+#pragma unroll 1
+      for (int g = warp; g * AZ::LPW < NX; g += nw) {
+        spec::wpass<NZ, AZ::R0, 1, false, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
+        spec::wsandwich<NZ, AZ::R1, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P}, msk);
+        spec::wpass<NZ, AZ::R0, AZ::R1, true, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
+      }
+    }
+    spec::fence_proxy_async();   // this thread's slab writes, before the bulk copies read them
+    __syncthreads();   // slab done (and the mask words free)
+    if (warp == 0) {
+      if (!bad) {
+        spec::fence_proxy_async();
+        cf* dst = slab(u);
+        for (int z = lane; z < NZ; z += 32)
+          spec::bulk_s2g(dst + (int64_t)z * PL, P + z * NX, NX * (unsigned)sizeof(cf));
+        spec::bulk_commit();
+      }
+      const int u2 = u + 2 * (int)gridDim.x;
+      if (u2 < units) {
+        spec::bulk_wait_read();   // this buffer's rows have left shared memory
+        __syncwarp();
+        rows_g2s(P, slab(u2), NZ, NX, PL, &bar[b]);
+      }
+    }
+  }
+  if (warp == 0) spec::bulk_wait_all();
+  if (__syncthreads_or(bad) && tid == 0) atomicOr(err, kErrWait);
+}
+
+// Inverse plane pass, persistent over units u = (cc fastest, then z, then f):
+// plane z of T[f][cc] by TMA, bDFT_y over the columns, bDFT_x over the rows,
+// × conj(S'_c), written back in place.
+template <class Sh>
+__global__ void __launch_bounds__(Sh::XYW * 32, 1)
+    k_padj(cf* __restrict__ T, int nf, int cc0, int ch, const cf* __restrict__ smod,
+           const cf* __restrict__ twx_g, const cf* __restrict__ twy_g, int* __restrict__ err) {
+  using AX = typename Sh::AX;
+  using AY = typename Sh::AY;
+  constexpr int NX = Sh::NX, NY = Sh::NY, NZ = Sh::NZ, PL = Sh::PL;
+  constexpr int64_t NVOX = Sh::NVOX;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  cf* P = reinterpret_cast<cf*>(smraw);
+  cf* W = P + PL;
+  cf* twx = W + PL;
+  cf* twy = twx + Sh::ev(NX);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(twy + Sh::ev(NY));
+  const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
+  const int units = ch * NZ * nf;
+  auto plane = [&](int u) {
+    const int cc = u % ch, r = u / ch, z = r % NZ, f = r / NZ;
+    return T + ((int64_t)f * ch + cc) * NVOX + (int64_t)z * PL;
+  };
+  if (tid == 0) {
+    spec::mbar_init(bar, 1);
+    spec::mbar_fence_init();
+  }
+  for (int i = tid; i < NX; i += blockDim.x) twx[i] = twx_g[i];
+  for (int i = tid; i < NY; i += blockDim.x) twy[i] = twy_g[i];
+  __syncthreads();
+  int u = blockIdx.x;
+  if (tid == 0 && u < units) {
+    spec::mbar_expect_tx(bar, PL * (unsigned)sizeof(cf));
+    spec::bulk_g2s(P, plane(u), PL * (unsigned)sizeof(cf), bar);
+  }
+  unsigned par = 0;
+  bool bad = false;
+  for (; u < units; u += gridDim.x) {
+    if (!bad && !spec::mbar_wait(bar, par)) bad = true;
+    par ^= 1u;
+    if (!bad) {
+#pragma unroll 1
+      for (int g = warp; g * AY::LPW < NX; g += nw) pa_cols<Sh>(P, W, twy, g * AY::LPW);
+    }
+    __syncthreads();   // columns done: P free
+    const int nxt = u + (int)gridDim.x;
+    if (tid == 0 && nxt < units) {
+      spec::fence_proxy_async();
+      spec::mbar_expect_tx(bar, PL * (unsigned)sizeof(cf));
+      spec::bulk_g2s(P, plane(nxt), PL * (unsigned)sizeof(cf), bar);
+    }
+    if (!bad) {
+      const int cc = u % ch, z = (u / ch) % NZ;
+      const cf* sc = smod + (int64_t)(cc0 + cc) * NVOX + (int64_t)z * PL;
+      cf* dst = plane(u);
+#pragma unroll 1
+      for (int g = warp; g * AX::LPW < NY; g += nw) pa_rows<Sh>(W, twx, g * AX::LPW, dst, sc);
+    }
+    __syncthreads();   // rows done: W free
+  }
+  if (__syncthreads_or(bad) && tid == 0) atomicOr(err, kErrWait);
+}
+
+// Coil combine of a chunk: out[t0 + f] (mode 0: scale·Σ − A'y when subtract,
+// else scale·Σ; mode 1: out += scale·Σ) with Σ over the ch coils of T[f] in
+// coil order.  Pairs of values per thread when every pointer is 16-byte aligned.
+__global__ void k_csum(const cf* __restrict__ T, int nf, int ch, int64_t nvox, cf* __restrict__ out,
+                       const cf* __restrict__ ahy, int t0, float scale, int mode, int subtract) {
+  const int64_t step = (int64_t)gridDim.x * blockDim.x;
+  const bool vec = ((reinterpret_cast<uintptr_t>(T) | reinterpret_cast<uintptr_t>(out) |
+                     reinterpret_cast<uintptr_t>(ahy)) & 15) == 0 && (nvox % 2) == 0;
+  if (vec) {
+    const int64_t h = nvox / 2, n2 = (int64_t)nf * h;
+    const float4* t4 = reinterpret_cast<const float4*>(T);
+    float4* o4 = reinterpret_cast<float4*>(out) + (int64_t)t0 * h;
+    const float4* a4 = reinterpret_cast<const float4*>(ahy) + (int64_t)t0 * h;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += step) {
+      const int64_t f = i / h, o = i - f * h;
+      const float4* src = t4 + f * ch * h + o;
+      float4 s = src[0];
+      for (int c = 1; c < ch; ++c) {
+        const float4 w = src[c * h];
+        s.x += w.x;
+        s.y += w.y;
+        s.z += w.z;
+        s.w += w.w;
+      }
+      float4 v = make_float4(s.x * scale, s.y * scale, s.z * scale, s.w * scale);
+      if (mode) {
+        const float4 g = o4[i];
+        v = make_float4(g.x + v.x, g.y + v.y, g.z + v.z, g.w + v.w);
+      } else if (subtract) {
+        const float4 a = a4[i];
+        v = make_float4(v.x - a.x, v.y - a.y, v.z - a.z, v.w - a.w);
+      }
+      o4[i] = v;
+    }
+    return;
+  }
+  const int64_t n = (int64_t)nf * nvox;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += step) {
+    const int64_t f = i / nvox, o = i - f * nvox;
+    const cf* src = T + f * ch * nvox + o;
+    cf s = src[0];
+    for (int c = 1; c < ch; ++c) s = cadd(s, src[c * nvox]);
+    const int64_t oi = (int64_t)t0 * nvox + i;
+    cf v = cscale(s, scale);
+    if (mode) v = cadd(out[oi], v);
+    else if (subtract) v = csub(v, ahy[oi]);
+    out[oi] = v;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Tensor-core plane pass (tcgen05).  The four 1-D transforms of a plane are
 // dense DFT products on the tensor cores: with F[n][k] = e^{−2πi nk/N} (zero
@@ -650,6 +1026,12 @@ struct SpecOps {
   const void* zadj;
   int zfwd_threads, xy_threads, zadj_threads;
   size_t smem_zfwd, smem_zadj, smem_xy;
+  // four-pass form
+  const void* pfwd;
+  const void* zmask;     // two CTAs per SM (64 registers)
+  const void* zmask1;    // one CTA per SM (more registers, MSLR_ZMASK_CTAS=1)
+  const void* padj;
+  size_t smem_pfwd, smem_zmask, smem_padj;
   const void* xy_tc;                       // tensor-core plane pass (square planes), or null
   size_t smem_xy_tc;
   std::vector<uint32_t> (*dft)();          // its DFT tiles
@@ -669,6 +1051,13 @@ SpecOps ops_of() {
             Sh::smem_zfwd,
             Sh::smem_zadj,
             Sh::smem_xy,
+            reinterpret_cast<const void*>(&k_pfwd<Sh>),
+            reinterpret_cast<const void*>(&k_zmask<Sh, 2>),
+            reinterpret_cast<const void*>(&k_zmask<Sh, 1>),
+            reinterpret_cast<const void*>(&k_padj<Sh>),
+            Sh::smem_pfwd,
+            Sh::smem_zmask,
+            Sh::smem_padj,
             nullptr,
             0,
             nullptr};
@@ -730,6 +1119,32 @@ bool sense_spec_setup(Ctx* c) {
     c->spec_fr = fr;
   }
   c->spec_zfwd_ctas = per_sm_z * c->nsm;
+  // four-pass form (default; MSLR_SENSE_PATH=3 keeps the three-kernel form)
+  {
+    const char* sp = std::getenv("MSLR_SENSE_PATH");
+    c->spec_four = !(sp && std::string(sp) == "3");
+  }
+  if (c->spec_four) {
+    const char* zc = std::getenv("MSLR_ZMASK_CTAS");
+    c->spec_zmask1 = zc && std::string(zc) == "1";
+    const void* zk = c->spec_zmask1 ? o->zmask1 : o->zmask;
+    int a = 0, b = 0, d = 0;
+    if (cudaFuncSetAttribute(o->pfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_pfwd) ||
+        cudaFuncSetAttribute(zk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zmask) ||
+        cudaFuncSetAttribute(o->padj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_padj) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, o->pfwd, o->xy_threads, o->smem_pfwd) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, zk, o->zadj_threads, o->smem_zmask) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, o->padj, o->xy_threads, o->smem_padj) ||
+        a < 1 || b < 1 || d < 1 ||
+        dalloc(c, (void**)&c->d_xsum, (size_t)c->Nt * c->nvox * sizeof(cf))) {
+      cudaGetLastError();
+      c->spec_four = false;
+    } else {
+      c->spec_pfwd_ctas = a * c->nsm;
+      c->spec_zmask_ctas = b * c->nsm;
+      c->spec_padj_ctas = d * c->nsm;
+    }
+  }
   // tensor-core plane pass only on request (MSLR_XY_PATH=tc): at 90×90 its
   // padded split-BF16 DFT products (12 MMAs of 128×96×16 per K step, four
   // products per plane, serialised with their epilogues) take longer than the
@@ -760,10 +1175,77 @@ static int prof_mark(Ctx* c, cudaStream_t st) {
   return MSLR_OK;
 }
 
+// Four-pass normal operator (see k_pfwd ... k_csum): Σ_k X_k once, then per
+// coil group and chunk of frames the four kernels.
+static int normal_op_four(Ctx* c, const SpecOps* o, const cf* X, int ns, int64_t sstride, cf* g,
+                          bool subtract, cudaStream_t st) {
+  const float scale = (float)(1.0 / (double)c->nvox);
+  const int Nc = c->Nc;
+  const int Ch = std::max(1, std::min(Nc, c->spec_ch));             // coils per group
+  int F = std::max(1, c->spec_fr);                                  // frames per chunk
+  while (F > 1 && (int64_t)F * Ch > (int64_t)c->F * Nc) --F;        // within the k-space buffer
+  const int64_t nvox = c->nvox;
+  // the summed image: X itself for one 16-byte aligned image, else Σ_k X_k
+  const cf* xs = X;
+  if (ns > 1 || (reinterpret_cast<uintptr_t>(X) & 15)) {
+    k_xsum<<<4 * c->nsm, 512, 0, st>>>(X, ns, sstride, c->d_xsum, (int64_t)c->Nt * nvox);
+    MSLR_CUDA_TRY(cudaGetLastError());
+    c->launches += 1;
+    xs = c->d_xsum;
+  }
+  int nwords = c->nwords;
+  const cf* smod = c->d_smaps_mod;
+  const uint32_t* mask = c->d_mask;
+  const cf* ahy = c->d_ahy;
+  cf* T = c->d_T;
+  int* err = c->d_err;
+  const int sub = subtract ? 1 : 0;
+  const void* zk = c->spec_zmask1 ? o->zmask1 : o->zmask;
+  c->prof_kernels = 4;
+  for (int cc0 = 0; cc0 < Nc; cc0 += Ch) {
+    int ch = std::min(Ch, Nc - cc0);
+    const int mode = cc0 > 0 ? 1 : 0;
+    for (int t0 = 0; t0 < c->Nt; t0 += F) {
+      int f = std::min(F, c->Nt - t0);
+      const int planes = ch * c->N[2] * f;
+      if (int rc = prof_mark(c, st)) return rc;
+      {
+        const int grid = std::max(1, std::min(planes, c->spec_pfwd_ctas));
+        void* args[] = {(void*)&xs, (void*)&t0, (void*)&f, (void*)&cc0, (void*)&ch, (void*)&smod,
+                        (void*)&T,  (void*)&c->d_tw[0], (void*)&c->d_tw[1], (void*)&err};
+        MSLR_CUDA_TRY(cudaLaunchKernel(o->pfwd, dim3(grid), dim3(o->xy_threads), args, o->smem_pfwd, st));
+      }
+      if (int rc = prof_mark(c, st)) return rc;
+      {
+        const int slabs = ch * f * c->N[1];
+        const int grid = std::max(1, std::min(slabs, c->spec_zmask_ctas));
+        void* args[] = {(void*)&T, (void*)&mask, (void*)&nwords, (void*)&t0, (void*)&f, (void*)&ch,
+                        (void*)&c->d_tw[2], (void*)&err};
+        MSLR_CUDA_TRY(cudaLaunchKernel(zk, dim3(grid), dim3(o->zadj_threads), args, o->smem_zmask, st));
+      }
+      if (int rc = prof_mark(c, st)) return rc;
+      {
+        const int grid = std::max(1, std::min(planes, c->spec_padj_ctas));
+        void* args[] = {(void*)&T,  (void*)&f, (void*)&cc0, (void*)&ch, (void*)&smod,
+                        (void*)&c->d_tw[0], (void*)&c->d_tw[1], (void*)&err};
+        MSLR_CUDA_TRY(cudaLaunchKernel(o->padj, dim3(grid), dim3(o->xy_threads), args, o->smem_padj, st));
+      }
+      if (int rc = prof_mark(c, st)) return rc;
+      k_csum<<<4 * c->nsm, 512, 0, st>>>(T, f, ch, nvox, g, ahy, t0, scale, mode, sub);
+      MSLR_CUDA_TRY(cudaGetLastError());
+      if (int rc = prof_mark(c, st)) return rc;
+      c->launches += 4;
+    }
+  }
+  return MSLR_OK;
+}
+
 int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool subtract,
                    cudaStream_t st) {
   const SpecOps* o = find_ops(c->N[0], c->N[1], c->N[2]);
   if (!o) return fail(MSLR_ERR_UNSUPPORTED, "no specialised SENSE kernels for this shape");
+  if (c->spec_four && !c->xy_tc) return normal_op_four(c, o, X, ns, sstride, g, subtract, st);
+  c->prof_kernels = 3;
   float scale = (float)(1.0 / (double)c->nvox);
   const int Nc = c->Nc, Ny = c->N[1], Nz = c->N[2];
   const int Ch = std::max(1, std::min(Nc, c->spec_ch));             // coils per group
