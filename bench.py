@@ -32,14 +32,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "metric"
-# DRAM bytes (read + write) per k-space plane of a plane-pass launch, from an
-# ncu capture of k_xy3 at 90×90×60 (dram__bytes_read.sum + dram__bytes_write.sum
-# of one launch of 4 frames × 6 coils × 60 planes; cold cache: ncu flushes L2
-# before the launch, so this is an upper bound; a launch's traffic grows with
-# its planes)
-PLANE_TRAFFIC_PER_PLANE = (94088448 + 44334336) / 1440
-# B200 FP32 FMA peak: 148 SMs × 128 lanes × 2 flops × 1.965 GHz (nominal)
-FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
+# each kernel of the SENSE chunk (6 coils x 4 frames at 90x90x60) from an ncu
+# capture of the committed command in profiles/; ncu flushes L2 before each
+# launch, so these are cold-cache upper bounds.  Empty until captured.
+TRAFFIC_PER_LAUNCH = {}
 
 
 def describe(pb) -> str:
@@ -52,6 +49,9 @@ def describe(pb) -> str:
 
 
 METRIC = "POGM iter/s (90x90x60, 18 coils, Nt=300, 2 scales)"
+# the bounded CPU sample, the same for cpu_baseline and the reference arm:
+# fractions of the frames, of the local patches and of the global patch's rows
+CPU_SAMPLE = (4 / 300, 12 / 486, 1 / 30)
 
 
 def load_problem(name: str, seed_offset: int = 0):
@@ -238,7 +238,7 @@ def run_reference(args):
     desc = ""
     cores = 1
     for i in range(args.warmup + args.steps):
-        s, desc, cores = cpu_sample_iteration(pb, 2 / 300, 6 / 486, 1 / 60, seed=i)
+        s, desc, cores = cpu_sample_iteration(pb, *CPU_SAMPLE, seed=i)
         if i >= args.warmup:
             secs.append(s)
     v = 1.0 / (sum(secs) / len(secs))
@@ -341,10 +341,12 @@ def main():
     phases = {"normal_op_ms": t_normal * 1e3, "svst_ms": [t * 1e3 for t in t_svst]}
     if args.phases:
         log("phases", json.dumps(phases))
-    # roofline of the dominant kernel: the plane pass of the SENSE normal operator
-    # (per-launch device time from events around every launch of one normal op)
+    # roofline: the dominant kernel of the iteration (the longest kernel of the
+    # SENSE normal operator's chunks, per-launch device time from events around
+    # every launch) and the whole iteration against Σ_steps max(bytes/BW, flops/peak)
     from mslr_recon_b200 import roofline as RL
     peaks = RL.peaks()
+    fp32_tflops = M.fp32_peak()
     Ns = len(pb["patch_sizes"])
     roof = None
     try:
@@ -352,37 +354,78 @@ def main():
     except Exception as exc:   # shapes without the specialised kernels
         kms, nl = None, 0
         log("no per-kernel profile:", exc)
+    ch = min(Nc, tuning["coils_per_group"])
+    fr = tuning["frames_per_chunk"]
     if kms:
         phases["normal_op_kernel_ms"] = kms
         phases["normal_op_launches_per_kernel"] = nl
-        # a chunk: one coil group × frames per chunk, every kz plane of each
-        planes_per_launch = Nz * min(Nc, tuning["coils_per_group"]) * tuning["frames_per_chunk"]
-        byts = RL.plane_pass_bytes(Nx, Ny, planes_per_launch)
-        fl = RL.plane_pass_flops(Nx, Ny, planes_per_launch)
-        tdom = kms["xy"] / 1e3
+    if kms and "pfwd" in kms:
+        per = RL.four_pass_kernels(pb["N"], ch, fr)
+        names = {"pfwd": "k_pfwd (forward plane pass: coil map x summed image, DFT_y, DFT_x)",
+                 "zmask": "k_zmask (z pass: DFT_z, k-space mask, inverse DFT_z)",
+                 "padj": "k_padj (inverse plane pass: inverse DFT_y, DFT_x, x conj(coil map))",
+                 "csum": "k_csum (coil combine into g)"}
+        dom = max(("pfwd", "zmask", "padj"), key=lambda k: kms[k])
+        tdom = kms[dom] / 1e3
+        byts, fl = per[dom]["bytes"], per[dom]["flops"]
         achieved = byts / tdom / 1e9
-        roof = {"bound": "hbm", "kernel": "k_xy3 (plane pass: DFT_x, DFT_y, mask, inverse)",
+        t_hbm, t_fp32 = byts / (peaks["hbm_gbs"] * 1e9), fl / (fp32_tflops * 1e12)
+        roof = {"bound": "hbm", "kernel": names[dom],
                 "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"],
-                "traffic": PLANE_TRAFFIC_PER_PLANE * planes_per_launch,
-                "algorithmic_bytes_per_launch": byts, "launch_ms": kms["xy"],
+                "traffic": TRAFFIC_PER_LAUNCH.get(dom),
+                "algorithmic_bytes_per_launch": byts, "launch_ms": kms[dom],
                 "peak_source": peaks["source"],
-                "fp32": {"achieved_tflops": fl / tdom / 1e12, "nominal_peak_tflops": FP32_NOMINAL_TFLOPS,
-                         "note": "FP32 SIMT FFT; nominal 5 N log2 N flops; peak is nominal, not measured"}}
+                "binding": "fp32" if t_fp32 > t_hbm else "hbm",
+                "fp32": {"achieved_tflops": fl / tdom / 1e12, "peak_tflops": fp32_tflops,
+                         "frac": fl / tdom / 1e12 / fp32_tflops,
+                         "note": "nominal 5 N log2 N FFT flops per launch; peak measured by the "
+                                 "library's FMA probe"},
+                "kernels": {k: {"launch_ms": kms[k], "bytes": per[k]["bytes"], "flops": per[k]["flops"],
+                                "hbm_frac": per[k]["bytes"] / (kms[k] / 1e3) / 1e9 / peaks["hbm_gbs"],
+                                "fp32_frac": per[k]["flops"] / (kms[k] / 1e3) / 1e12 / fp32_tflops}
+                            for k in per}}
     else:
         byts = RL.normal_op_bytes(nvox, Nt, Nc, Ns)
         achieved = byts / t_normal / 1e9
         roof = {"bound": "hbm", "kernel": "normal_op", "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                 "algorithmic_bytes": byts, "peak_source": peaks["source"]}
+    scales = []
+    for ps_, ss_ in zip(pb["patch_sizes"], pb["strides"]):
+        gg = [min(a, b) for a, b in zip(ps_, pb["N"])]
+        nst = [-(-(n - p_) // s_) + 1 for n, p_, s_ in zip(pb["N"], gg, ss_)]
+        scales.append((gg[0] * gg[1] * gg[2], nst[0] * nst[1] * nst[2]))
+    steps_ = RL.iteration_steps(pb["N"], Nt, Nc, scales)
+    t_bound = RL.iteration_bound_seconds(steps_, peaks["hbm_gbs"], fp32_tflops, peaks["bf16_tflops_sustained"])
+    t_iter = secs / args.steps
+    roof["iteration_frac"] = t_bound / t_iter
+    roof["iteration_bound_ms"] = t_bound * 1e3
+    roof["iteration_note"] = ("sum over steps (normal operator, update, per scale the split-BF16 Gram/W/"
+                              "rebuild products at a third of the sustained BF16 peak and the eigen stage "
+                              "on the measured FP32 peak) of max(bytes/HBM, flops/peak), over the measured "
+                              "iteration time")
 
     plain_ips = None
+    plain_phases = None
     if not args.no_plain and args.form == "tuned":
         del ctx
         torch.cuda.empty_cache()
-        pctx, pX, psecs, _, _ = device_run("plain", max(2, args.steps // 2), 1)
-        plain_ips = world * max(2, args.steps // 2) / psecs
-        del pctx, pX
+        psteps = max(2, args.steps // 2)
+        pctx, pX, psecs, _, _ = device_run("plain", psteps, 1)
+        plain_ips = world * psteps / psecs
+        pg = torch.empty((Nt, Nz, Ny, Nx), dtype=torch.complex64, device=dev)
+        pt_normal = ev_time(lambda: pctx.normal(pX, out=pg), reps=1)
+        ptmp = torch.empty_like(pg)
+        pt_svst = [ev_time(lambda k=k: pctx.patch_svst(k, 0.9 * pctx.lambdas[k], pX[k], out=ptmp), reps=1)
+                   for k in range(pctx.Ns)]
+        plain_ms = 1e3 * psecs / psteps
+        plain_phases = {"iteration_ms": plain_ms, "normal_op_ms": pt_normal * 1e3,
+                        "svst_ms": [t * 1e3 for t in pt_svst],
+                        # the plain form with the tuned form's SENSE operator, from the two
+                        # forms' measured phases: plain iteration − plain normal op + tuned normal op
+                        "iteration_with_tuned_sense_ms": plain_ms - pt_normal * 1e3 + t_normal * 1e3}
+        del pctx, pX, pg, ptmp
     else:
         del ctx
     torch.cuda.empty_cache()
@@ -422,7 +465,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        s, desc, cores = cpu_sample_iteration(pb, 4 / 300, 12 / 486, 1 / 30)
+        s, desc, cores = cpu_sample_iteration(pb, *CPU_SAMPLE)
         cpu = {"value": 1.0 / s, "unit": "iter/s", "cores": cores, "kind": "port", "sample": desc}
 
     if world > 1:
@@ -438,7 +481,10 @@ def main():
                            "l2": f"inputs larger than L2 (X is {pb['y'].shape[0] * nvox * 8 * len(pb['patch_sizes']) / 1e9:.1f} GB)",
                            "plain_form_iter_s": plain_ips,
                            "tuned_over_plain": (value / world / plain_ips * world) if plain_ips else None,
-                           "phases": phases},
+                           "tuned_over_plain_with_tuned_sense":
+                               (plain_phases["iteration_with_tuned_sense_ms"] / (1e3 * secs / args.steps))
+                               if plain_phases else None,
+                           "phases": phases, "plain_phases": plain_phases},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)

@@ -316,6 +316,12 @@ int mslr_launch_count(const mslr_ctx* ctx, uint64_t* count);
 int mslr_power_iter(mslr_ctx* ctx, int32_t niter, double tol, double* sigma1,
                     int32_t* iters_done, void* stream);
 
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (the best of
+ * three timed launches of independent FMA chains on every SM), the
+ * denominator of the roofline fractions of SIMT-bound kernels.  No
+ * counterpart in the reference.  Synchronises `stream`. */
+int mslr_fp32_peak(double* tflops, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -71,6 +71,7 @@ SIGNATURES = {
                                       C.POINTER(C.c_double), C.POINTER(C.c_double), _P]),
     "mslr_sync": (C.c_int, [_P, _P]),
     "mslr_set_wait_limit": (C.c_int, [_P, _I64]),
+    "mslr_fp32_peak": (C.c_int, [C.POINTER(C.c_double), _P]),
     "mslr_svst_batch_noalloc": (C.c_int, [_I32, _I32, _I32, C.POINTER(C.c_double), _P, _P, _P]),
 }
 

@@ -63,6 +63,13 @@ def sampling(ksp: torch.Tensor, idx=None, y=None, stream=None) -> int:
     return int(K.value)
 
 
+def fp32_peak(stream=None) -> float:
+    """Measured FP32 FMA throughput of the current device, TFLOP/s."""
+    v = C.c_double()
+    check(lib.mslr_fp32_peak(C.byref(v), _stream_ptr(stream)))
+    return float(v.value)
+
+
 class MSLRContext:
     """One reconstruction context.
 
