@@ -154,9 +154,15 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # CPU port (oracle restatement in FP32, all host threads) — bounded sample
 # ---------------------------------------------------------------------------
-def cpu_sample_iteration(pb, frac_frames: float, frac_patches: float, frac_rows: float, seed=0):
+def cpu_sample_iteration(pb, frac_frames: float, frac_patches: float, frac_rows: float, seed=0,
+                         costs: dict | None = None):
     """Time a bounded sample of one POGM iteration of the CPU port and scale
-    it to a full iteration.  Returns (seconds_per_iteration, description)."""
+    it to a full iteration.  Returns (seconds_per_iteration, description,
+    threads).  With ``costs`` (a dict) it also times, on the same sample, the
+    cost evaluations the reference's pogm_mod and logger add to every
+    iteration — Fcost and the logger each run dc_cost (one forward SENSE) and
+    reg_cost (svdvals of every patch of every scale) — and stores their
+    scaled seconds per iteration under costs["seconds"]."""
     from concurrent.futures import ThreadPoolExecutor
 
     from oracle import mslr_oracle as O
@@ -206,6 +212,22 @@ def cpu_sample_iteration(pb, frac_frames: float, frac_patches: float, frac_rows:
     float(np.sum(np.real(-gg[None] * (un - us)), dtype=np.float64))
     td = (time.perf_counter() - t0) * nvox / nrow
     del zn
+    if costs is not None:
+        # dc_cost: A Σ_k X_k − y on the sampled frames; reg_cost: svdvals of the
+        # sampled local patches and of the global patch's row subset; twice
+        t0 = time.perf_counter()
+        for t in range(nf):
+            O.sense_forward_frame(x[t], smaps, idx[t], workers=ncores) - y[t]
+        tfa = (time.perf_counter() - t0) * Nt / nf
+        import scipy.linalg as sla
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(ncores) as ex:
+            list(ex.map(lambda m: sla.svdvals(m, check_finite=False), mats))
+        tfb = (time.perf_counter() - t0) * g.Np / npatch
+        t0 = time.perf_counter()
+        sla.svdvals(G, check_finite=False)
+        tfc = (time.perf_counter() - t0) * nvox / nrow
+        costs["seconds"] = 2.0 * (tfa + tfb + tfc)
     total = ta + tb + tc + td
     desc = (f"FP32 numpy/scipy port, {ncores} threads: normal op on {nf}/{Nt} frames, gesdd SVST on "
             f"{npatch}/{g.Np} 10^3 patches, global-patch SVD on {nrow}/{nvox} rows, POGM update on "
@@ -465,8 +487,12 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        s, desc, cores = cpu_sample_iteration(pb, *CPU_SAMPLE)
-        cpu = {"value": 1.0 / s, "unit": "iter/s", "cores": cores, "kind": "port", "sample": desc}
+        extra = {}
+        s, desc, cores = cpu_sample_iteration(pb, *CPU_SAMPLE, costs=extra)
+        cpu = {"value": 1.0 / s, "unit": "iter/s", "cores": cores, "kind": "port", "sample": desc,
+               "as_reference_iter_s": 1.0 / (s + extra["seconds"]),
+               "as_reference_note": "with the per-iteration Fcost and logger cost evaluations the "
+                                    "reference runs (2 forward SENSE passes and 2 svdvals sweeps)"}
 
     if world > 1:
         dist.barrier()
