@@ -250,6 +250,42 @@ int mslr_sync(mslr_ctx* ctx, void* stream);
  * A small value exists to test that path; 0 makes every such wait give up. */
 int mslr_set_wait_limit(mslr_ctx* ctx, int64_t polls);
 
+/* ------------------------------------------------------------------------
+ * Sharded iteration over several GPUs (no counterpart in the reference, which
+ * runs on one device).  One process per GPU; each rank holds a context for
+ * its block of frames (the SENSE normal operator and the POGM state) and a
+ * context for its z-slab of the volume (patch SVST over all frames).  Per
+ * iteration (mslr-recon_b200/sharded.py drives it over torch.distributed):
+ *   mslr_pogm_step_local   g = A'(A Σ_k x_k − y) on the rank's frames, the
+ *                          momentum scalars, u, and z into Z (Ns, Nt_rank,
+ *                          nvox); the rank's restart totals into sums_dev
+ *                          (4 doubles on the device: Σ Re(−g·Δu), Σ|g|²,
+ *                          Σ|Δu|², Σ Re(g·gold)) — no decision yet;
+ *   (the caller sums sums_dev over the ranks)
+ *   mslr_pogm_step_decide  the restart decision and t/σ update from the
+ *                          totals (src/mirt_mod.jl:163-184), identical on
+ *                          every rank;
+ *   mslr_pogm_scalars      α, β, γ, ζ of the iteration to the host
+ *                          (synchronises `stream`): the caller's thresholds
+ *                          are ζ·λ_k;
+ *   (the caller moves z from frames to slabs, all-to-all)
+ *   mslr_patch_svst        on the slab for a scale that tiles it;
+ *   mslr_patch_gram        for the global patch: the slab's partial Gram
+ *                          (n × n, column-major; a tall patch's Gram Pᴴ P is
+ *                          a sum over voxels), summed over the ranks by the
+ *                          caller, then
+ *   mslr_patch_svst_gram   SVST of the slab's rows of that patch from the
+ *                          summed Gram (eigen stage, W, rebuild);
+ *   (the caller moves x from slabs back to frames, all-to-all).
+ * mslr_patch_gram / mslr_patch_svst_gram need a single-patch scale.
+ * ------------------------------------------------------------------------ */
+int mslr_pogm_step_local(mslr_ctx* ctx, void* X, void* Z, double* sums_dev, void* stream);
+int mslr_pogm_step_decide(mslr_ctx* ctx, const double* sums_dev, void* stream);
+int mslr_pogm_scalars(mslr_ctx* ctx, double* alpha_beta_gamma_zeta, void* stream);
+int mslr_patch_gram(mslr_ctx* ctx, int32_t scale, const void* img, void* gram, void* stream);
+int mslr_patch_svst_gram(mslr_ctx* ctx, int32_t scale, double beta, const void* gram, const void* img_in,
+                         void* img_out, void* stream);
+
 /* Set-up of run_recon's inputs on the device (scripts/reconstruct.jl:86-147).
  *
  * mslr_sos_normalize: smaps_out = S ./ (sqrt.(sum(abs2.(S); dims=4)) .+ eps(Float32))

@@ -72,6 +72,11 @@ SIGNATURES = {
     "mslr_sync": (C.c_int, [_P, _P]),
     "mslr_set_wait_limit": (C.c_int, [_P, _I64]),
     "mslr_fp32_peak": (C.c_int, [C.POINTER(C.c_double), _P]),
+    "mslr_pogm_step_local": (C.c_int, [_P, _P, _P, _P, _P]),
+    "mslr_pogm_step_decide": (C.c_int, [_P, _P, _P]),
+    "mslr_pogm_scalars": (C.c_int, [_P, C.POINTER(C.c_double), _P]),
+    "mslr_patch_gram": (C.c_int, [_P, _I32, _P, _P, _P]),
+    "mslr_patch_svst_gram": (C.c_int, [_P, _I32, _D, _P, _P, _P, _P]),
     "mslr_svst_batch_noalloc": (C.c_int, [_I32, _I32, _I32, C.POINTER(C.c_double), _P, _P, _P]),
 }
 

@@ -462,6 +462,53 @@ int mslr_pogm_run_costs(mslr_ctx* ctx, void* X, int32_t niter, double L, double 
   return MSLR_OK;
 }
 
+int mslr_pogm_step_local(mslr_ctx* ctx, void* X, void* Z, double* sums_dev, void* stream) {
+  CTX_CHECK(ctx);
+  NEED_BOUND(ctx);
+  if (!ctx->pogm_ready) return ctx_fail(ctx, fail(MSLR_ERR_STATE, "mslr_pogm_begin not called"));
+  if (!X || !Z || !sums_dev) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "null argument"));
+  CTX_RET(ctx, pogm_step_local(ctx, reinterpret_cast<cf*>(X), reinterpret_cast<cf*>(Z), sums_dev,
+                               reinterpret_cast<cudaStream_t>(stream)));
+  return MSLR_OK;
+}
+
+int mslr_pogm_step_decide(mslr_ctx* ctx, const double* sums_dev, void* stream) {
+  CTX_CHECK(ctx);
+  if (!ctx->pogm_ready) return ctx_fail(ctx, fail(MSLR_ERR_STATE, "mslr_pogm_begin not called"));
+  if (!sums_dev) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "null argument"));
+  CTX_RET(ctx, pogm_step_decide(ctx, sums_dev, reinterpret_cast<cudaStream_t>(stream)));
+  return MSLR_OK;
+}
+
+int mslr_pogm_scalars(mslr_ctx* ctx, double* alpha_beta_gamma_zeta, void* stream) {
+  CTX_CHECK(ctx);
+  if (!ctx->pogm_ready) return ctx_fail(ctx, fail(MSLR_ERR_STATE, "mslr_pogm_begin not called"));
+  if (!alpha_beta_gamma_zeta) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "null argument"));
+  CTX_RET(ctx, pogm_scalars(ctx, alpha_beta_gamma_zeta, reinterpret_cast<cudaStream_t>(stream)));
+  return MSLR_OK;
+}
+
+int mslr_patch_gram(mslr_ctx* ctx, int32_t scale, const void* img, void* gram, void* stream) {
+  CTX_CHECK(ctx);
+  if (scale < 0 || scale >= ctx->Ns || !img || !gram) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad argument"));
+  CTX_RET(ctx, patch_gram_out(ctx, scale, reinterpret_cast<const cf*>(img), reinterpret_cast<cf*>(gram),
+                              reinterpret_cast<cudaStream_t>(stream)));
+  return MSLR_OK;
+}
+
+int mslr_patch_svst_gram(mslr_ctx* ctx, int32_t scale, double beta, const void* gram, const void* img_in,
+                         void* img_out, void* stream) {
+  CTX_CHECK(ctx);
+  if (scale < 0 || scale >= ctx->Ns || !gram || !img_in || !img_out)
+    return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad argument"));
+  if (!(beta >= 0.0) || !std::isfinite(beta))
+    return ctx_fail(ctx, fail(MSLR_ERR_ARG, "beta must be finite and non-negative"));
+  CTX_RET(ctx, patch_svst_from_gram(ctx, scale, beta, reinterpret_cast<const cf*>(gram),
+                                    reinterpret_cast<const cf*>(img_in), reinterpret_cast<cf*>(img_out),
+                                    reinterpret_cast<cudaStream_t>(stream)));
+  return MSLR_OK;
+}
+
 int mslr_autotune(mslr_ctx* ctx, void* stream) {
   CTX_CHECK(ctx);
   NEED_BOUND(ctx);

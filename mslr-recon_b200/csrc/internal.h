@@ -224,6 +224,14 @@ int dc_cost_eval(Ctx* c, const cf* X, int ns, double* dc_out, cudaStream_t st);
 int pogm_setup(Ctx* c);
 int pogm_begin(Ctx* c, cf* X, int niter, double L, double cutoff, double bsig, cudaStream_t st);
 int pogm_step(Ctx* c, cf* X, cudaStream_t st);
+// sharded iteration (sharded.py): the rank-local half, the decision from the
+// totals over the ranks, the current scalars
+int pogm_step_local(Ctx* c, cf* X, cf* Zout, double* sums_dev, cudaStream_t st);
+int pogm_step_decide(Ctx* c, const double* sums_dev, cudaStream_t st);
+int pogm_scalars(Ctx* c, double* out, cudaStream_t st);
+int patch_gram_out(Ctx* c, int s, const cf* img, cf* gram_out, cudaStream_t st);
+int patch_svst_from_gram(Ctx* c, int s, double beta, const cf* gram, const cf* img_in, cf* img_out,
+                         cudaStream_t st);
 int init_x0(Ctx* c, cf* X, cudaStream_t st);
 int power_iter(Ctx* c, int niter, double tol, double* sigma1, int* iters, cudaStream_t st);
 int set_scalar(double* dst, double v, cudaStream_t st);

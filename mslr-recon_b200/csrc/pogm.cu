@@ -135,16 +135,9 @@ __global__ void __launch_bounds__(kRedThreads)
   if (threadIdx.x == 0) part[blockIdx.x * 4 + 3] = v;
 }
 
-// Restart decision and t/σ update (src/mirt_mod.jl:163-184).
-__global__ void k_pogm_finish(PogmState* s, const double* __restrict__ part, int nblocks,
-                              int ns, uint8_t* restarts, int32_t* err) {
-  __shared__ double sh[32];
-  double acc[4] = {0, 0, 0, 0};
-  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-    for (int q = 0; q < 4; ++q) acc[q] += part[b * 4 + q];
-  double tot[4];
-  for (int q = 0; q < 4; ++q) tot[q] = block_sum(acc[q], sh);
-  if (threadIdx.x != 0) return;
+// Restart decision and t/σ update (src/mirt_mod.jl:163-184) from the
+// iteration's totals tot = (Σ Re(−g·Δu), Σ|g|², Σ|Δu|², Σ Re(g·gold)).
+__device__ void pogm_decide(PogmState* s, const double* tot, int ns, uint8_t* restarts, int32_t* err) {
   const double dot = tot[0];
   const double gnorm = sqrt((double)ns * tot[1]);   // ‖Fgrad‖ of the replicated 5-D gradient
   const double dnorm = sqrt(tot[2]);
@@ -163,6 +156,40 @@ __global__ void k_pogm_finish(PogmState* s, const double* __restrict__ part, int
   restarts[s->iter] = (uint8_t)restart;
   s->told = tnew;
   s->iter += 1;
+}
+
+// The partial sums of k_pogm_update's blocks added in block order.
+__device__ void pogm_totals(const double* __restrict__ part, int nblocks, double* sh, double* tot) {
+  double acc[4] = {0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+    for (int q = 0; q < 4; ++q) acc[q] += part[b * 4 + q];
+  for (int q = 0; q < 4; ++q) tot[q] = block_sum(acc[q], sh);
+}
+
+__global__ void k_pogm_finish(PogmState* s, const double* __restrict__ part, int nblocks,
+                              int ns, uint8_t* restarts, int32_t* err) {
+  __shared__ double sh[32];
+  double tot[4];
+  pogm_totals(part, nblocks, sh, tot);
+  if (threadIdx.x == 0) pogm_decide(s, tot, ns, restarts, err);
+}
+
+// Sharded iteration: this rank's totals into sums (4 doubles, device), to be
+// added over the ranks by the caller before k_pogm_decide_sums.
+__global__ void k_pogm_reduce(const double* __restrict__ part, int nblocks, double* sums) {
+  __shared__ double sh[32];
+  double tot[4];
+  pogm_totals(part, nblocks, sh, tot);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 4; ++q) sums[q] = tot[q];
+}
+
+__global__ void k_pogm_decide_sums(PogmState* s, const double* __restrict__ sums, int ns,
+                                   uint8_t* restarts, int32_t* err) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double tot[4];
+  for (int q = 0; q < 4; ++q) tot[q] = sums[q];
+  pogm_decide(s, tot, ns, restarts, err);
 }
 
 __global__ void k_pogm_init(PogmState* s, double L, int niter, double cutoff, double bsig,
@@ -292,6 +319,44 @@ static int pogm_step_body(Ctx* c, cf* X, cudaStream_t st) {
     if ((rc = patch_svst(c, k, c->d_thr, c->lambdas[k], c->d_Z + k * E, X + k * E, st)))
       return rc;
   }
+  return MSLR_OK;
+}
+
+// Sharded iteration, first half on this rank's frames: g = A'(A Σ_k x_k − y),
+// the momentum scalars, u and z (z into Zout, (Ns, Nt, nvox) of this
+// context's frames) and this rank's restart totals into sums_dev (4 doubles).
+// The caller adds sums_dev over the ranks, then calls pogm_step_decide.
+int pogm_step_local(Ctx* c, cf* X, cf* Zout, double* sums_dev, cudaStream_t st) {
+  int rc;
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  if ((rc = normal_op(c, X, c->Ns, E, c->d_G, true, st))) return rc;
+  k_pogm_prepare<<<1, 32, 0, st>>>(c->d_state, c->d_thr);
+  k_pogm_update<<<kRedBlocks, kRedThreads, 0, st>>>(X, c->d_U, c->d_G, c->d_Gold, Zout, E, c->Ns,
+                                                    c->d_state, c->d_part);
+  k_pogm_reduce<<<1, kRedThreads, 0, st>>>(c->d_part, kRedBlocks, sums_dev);
+  MSLR_CUDA_TRY(cudaGetLastError());
+  c->launches += 3;
+  return MSLR_OK;
+}
+
+// Restart decision and t/σ update of a sharded iteration from the totals
+// over all ranks.
+int pogm_step_decide(Ctx* c, const double* sums_dev, cudaStream_t st) {
+  k_pogm_decide_sums<<<1, 32, 0, st>>>(c->d_state, sums_dev, c->Ns, c->d_restarts, c->d_err);
+  MSLR_CUDA_TRY(cudaGetLastError());
+  c->launches += 1;
+  return MSLR_OK;
+}
+
+// α, β, γ, ζ of the current iteration (after pogm_step_local).  Synchronises st.
+int pogm_scalars(Ctx* c, double* out, cudaStream_t st) {
+  PogmState h;
+  MSLR_CUDA_TRY(cudaMemcpyAsync(&h, c->d_state, sizeof(PogmState), cudaMemcpyDeviceToHost, st));
+  MSLR_CUDA_TRY(cudaStreamSynchronize(st));
+  out[0] = h.alpha;
+  out[1] = h.beta;
+  out[2] = h.gamma;
+  out[3] = h.zeta;
   return MSLR_OK;
 }
 

@@ -548,6 +548,56 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
   return MSLR_OK;
 }
 
+// The Gram matrix (n × n, column-major) of the one patch of a single-patch
+// scale s of img, into gram_out.  Sharded reconstructions add these partial
+// Grams over the ranks' slabs of a tall global patch (G = Pᴴ P is a sum over
+// voxels) and hand the sum to patch_svst_from_gram.
+int patch_gram_out(Ctx* c, int s, const cf* img, cf* gram_out, cudaStream_t st) {
+  const ScaleGeom& g = c->scales[s];
+  if (g.Np != 1) return fail(MSLR_ERR_ARG, "the scale has more than one patch");
+  const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
+  const int nsplit = split_of(g);
+  WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? s : 0].gram, g.Np, g.n, nsplit);
+  int rc;
+  if ((rc = svst_gram(img, m, 1, w, nsplit, c->tc_mode(), ctx_wait(c), st, &c->launches))) return rc;
+  MSLR_CUDA_TRY(cudaMemcpyAsync(gram_out, w.gram, (size_t)g.n * g.n * sizeof(cf), cudaMemcpyDeviceToDevice,
+                                st));
+  return MSLR_OK;
+}
+
+// SVST of the one patch of a single-patch scale s with threshold beta from a
+// given Gram matrix (n × n, column-major): eigen stage, W, rebuild of
+// img_in's patch into img_out (img_in may equal img_out).
+int patch_svst_from_gram(Ctx* c, int s, double beta, const cf* gram, const cf* img_in, cf* img_out,
+                         cudaStream_t st) {
+  const ScaleGeom& g = c->scales[s];
+  if (g.Np != 1) return fail(MSLR_ERR_ARG, "the scale has more than one patch");
+  const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
+  WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? s : 0].gram, 1, g.n, split_of(g));
+  const int tc = c->tc_mode();
+  int rc;
+  if ((rc = set_scalar(c->d_thr + 1, beta, st))) return rc;
+  MSLR_CUDA_TRY(cudaMemcpyAsync(w.gram, gram, (size_t)g.n * g.n * sizeof(cf), cudaMemcpyDeviceToDevice, st));
+  if ((rc = eig2_launch(g.n, 1, w.gram, reinterpret_cast<cf*>(w.zv), reinterpret_cast<float*>(w.aux), w.rank,
+                        c->d_thr + 1, 0, 1.0, st)))
+    return rc;
+  if ((rc = svst_form_w(w, g.n, 1, tc, ctx_wait(c), st, &c->launches))) return rc;
+  c->launches += 1;
+  cf* dst = g.partition ? img_out : c->d_pbuf;
+  if (g.partition && img_in == img_out) dst = c->d_img_tmp;
+  if ((rc = svst_rebuild(img_in, m, 1, w, dst, g.partition ? 1 : 0, tc, ctx_wait(c), st, &c->launches)))
+    return rc;
+  if (!g.partition) {
+    k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, img_out);
+    MSLR_CUDA_TRY(cudaGetLastError());
+    c->launches += 1;
+  } else if (dst != img_out) {
+    MSLR_CUDA_TRY(cudaMemcpyAsync(img_out, dst, (size_t)c->Nt * c->nvox * sizeof(cf), cudaMemcpyDeviceToDevice,
+                                  st));
+  }
+  return MSLR_OK;
+}
+
 // g_prox of run_recon (scripts/reconstruct.jl:196-202) for every scale at once:
 // Grams of all scales, one eigen launch per CTA variant over every patch of
 // every scale (the global patch's eigensolve overlaps the local patches'),
