@@ -1324,7 +1324,11 @@ int normal_op_spec(Ctx* c, const cf* X, int ns, int64_t sstride, cf* g, bool sub
 // Ch ≤ 8.
 int tune_sense_chunks(Ctx* c, cudaStream_t st) {
   if (!c->spec) return MSLR_OK;
-  const int chs[] = {2, 3, 4, 6, 8};
+  // the three-kernel form's clusters hold one coil per CTA (at most 8); the
+  // four-pass form takes any group size
+  const bool four = c->spec_four && !c->xy_tc;
+  std::vector<int> chs = {2, 3, 4, 6, 8};
+  if (four) chs.insert(chs.end(), {9, 12, 18});
   const int64_t E = (int64_t)c->Nt * c->nvox;
   float best = 1e30f;
   int bch = c->spec_ch, bfr = c->spec_fr;
