@@ -191,8 +191,9 @@ def cpu_sample_iteration(pb, frac_frames: float, frac_patches: float, frac_rows:
         blk = x[:, sz:sz + ps[2], sy:sy + ps[1], sx:sx + ps[0]].reshape(Nt, -1).T.copy()
         mats.append(blk)
     lam = O.ong_lustig_lambdas(pb["N"], Nt, pb["patch_sizes"])
+    from threadpoolctl import threadpool_limits
     t0 = time.perf_counter()
-    with ThreadPoolExecutor(ncores) as ex:
+    with threadpool_limits(1, "blas"), ThreadPoolExecutor(ncores) as ex:   # one patch per thread
         list(ex.map(lambda m: O.svst(m, lam[1]), mats))
     tb = (time.perf_counter() - t0) * g.Np / npatch
     # (c) global patch: thin SVD cost is linear in rows — time a row subset
@@ -200,7 +201,8 @@ def cpu_sample_iteration(pb, frac_frames: float, frac_patches: float, frac_rows:
     nrow = max(Nt, int(round(frac_rows * nvox)))
     G = x.reshape(Nt, nvox)[:, :nrow].T.copy()
     t0 = time.perf_counter()
-    O.svst(G, lam[0])
+    with threadpool_limits(ncores, "blas"):
+        O.svst(G, lam[0])
     tc = (time.perf_counter() - t0) * nvox / nrow
     # (d) POGM elementwise on the same row subset, two scales
     xs = np.stack([x.reshape(Nt, nvox)[:, :nrow]] * 2)
@@ -219,13 +221,13 @@ def cpu_sample_iteration(pb, frac_frames: float, frac_patches: float, frac_rows:
         for t in range(nf):
             O.sense_forward_frame(x[t], smaps, idx[t], workers=ncores) - y[t]
         tfa = (time.perf_counter() - t0) * Nt / nf
-        import scipy.linalg as sla
         t0 = time.perf_counter()
-        with ThreadPoolExecutor(ncores) as ex:
-            list(ex.map(lambda m: sla.svdvals(m, check_finite=False), mats))
+        with threadpool_limits(1, "blas"), ThreadPoolExecutor(ncores) as ex:
+            list(ex.map(lambda m: np.linalg.svd(m, compute_uv=False), mats))
         tfb = (time.perf_counter() - t0) * g.Np / npatch
         t0 = time.perf_counter()
-        sla.svdvals(G, check_finite=False)
+        with threadpool_limits(ncores, "blas"):
+            np.linalg.svd(G, compute_uv=False)
         tfc = (time.perf_counter() - t0) * nvox / nrow
         costs["seconds"] = 2.0 * (tfa + tfb + tfc)
     total = ta + tb + tc + td

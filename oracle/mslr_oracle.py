@@ -154,9 +154,11 @@ def coverage_count(N, patch_size, stride_size) -> np.ndarray:
 # SVST — src/recon.jl:183-211, loops :217-269
 # ---------------------------------------------------------------------------
 def _svd(X: np.ndarray):
-    """gesdd with a gesvd fallback, as src/recon.jl:189-193."""
+    """gesdd with a gesvd fallback, as src/recon.jl:189-193.  numpy's thin SVD
+    is LAPACK gesdd and runs without the interpreter lock, so patches in a
+    thread pool run concurrently; scipy's gesvd is the fallback."""
     try:
-        return sla.svd(X, full_matrices=False, lapack_driver="gesdd", check_finite=False)
+        return np.linalg.svd(X, full_matrices=False)
     except (np.linalg.LinAlgError, ValueError):
         return sla.svd(X, full_matrices=False, lapack_driver="gesvd", check_finite=False)
 
