@@ -70,6 +70,9 @@ static void free_ctx(mslr_ctx* c) {
   if (c->d_gbuf) cudaFree(c->d_gbuf);
   if (c->d_vjpw) cudaFree(c->d_vjpw);
   if (c->d_xsum) cudaFree(c->d_xsum);
+  if (c->sn_stream) cudaStreamDestroy(c->sn_stream);
+  if (c->sn_fork) cudaEventDestroy(c->sn_fork);
+  if (c->sn_join) cudaEventDestroy(c->sn_join);
   delete c;
 }
 

@@ -97,6 +97,12 @@ struct Ctx {
   bool spec_four = true;
   int spec_pfwd_ctas = 0, spec_zmask_ctas = 0, spec_padj_ctas = 0;
   bool spec_zmask1 = false;   // z-mask kernel variant with one CTA per SM
+  // chunks of the four-pass form alternate between two streams ("lanes",
+  // each with its own k-space buffer) when spec_lanes == 2, so one chunk's
+  // kernels overlap the other's
+  int spec_lanes = 1;
+  cudaStream_t sn_stream = nullptr;
+  cudaEvent_t sn_fork = nullptr, sn_join = nullptr;
   cf* d_xsum = nullptr;   // (Nt, nvox)
   bool xy_tc = false;     // tensor-core plane pass (DFT products on tcgen05)
   uint32_t* d_dft = nullptr;   // its split-BF16 DFT matrix tiles

@@ -1143,6 +1143,13 @@ bool sense_spec_setup(Ctx* c) {
       c->spec_pfwd_ctas = a * c->nsm;
       c->spec_zmask_ctas = b * c->nsm;
       c->spec_padj_ctas = d * c->nsm;
+      const char* ln = std::getenv("MSLR_SENSE_LANES");
+      if (ln && std::string(ln) == "2" &&
+          !cudaStreamCreateWithFlags(&c->sn_stream, cudaStreamNonBlocking) &&
+          !cudaEventCreateWithFlags(&c->sn_fork, cudaEventDisableTiming) &&
+          !cudaEventCreateWithFlags(&c->sn_join, cudaEventDisableTiming))
+        c->spec_lanes = 2;
+      cudaGetLastError();
     }
   }
   // tensor-core plane pass only on request (MSLR_XY_PATH=tc): at 90×90 its
@@ -1202,11 +1209,26 @@ static int normal_op_four(Ctx* c, const SpecOps* o, const cf* X, int ns, int64_t
   const int sub = subtract ? 1 : 0;
   const void* zk = c->spec_zmask1 ? o->zmask1 : o->zmask;
   c->prof_kernels = 4;
+  // two lanes: chunk j of every group on lane j % 2 (so the += of later
+  // groups stays ordered after the first group's chunk of the same frames),
+  // each lane with its own k-space buffer
+  const int64_t chunk_imgs = (int64_t)F * Ch;
+  const bool lanes = c->spec_lanes == 2 && !c->prof_on && 2 * chunk_imgs <= (int64_t)c->F * Nc &&
+                     c->Nt > F;
+  cudaStream_t side = c->sn_stream;
+  if (lanes) {
+    MSLR_CUDA_TRY(cudaEventRecord(c->sn_fork, st));
+    MSLR_CUDA_TRY(cudaStreamWaitEvent(side, c->sn_fork, 0));
+  }
+  cudaStream_t st0 = st;
   for (int cc0 = 0; cc0 < Nc; cc0 += Ch) {
     int ch = std::min(Ch, Nc - cc0);
     const int mode = cc0 > 0 ? 1 : 0;
-    for (int t0 = 0; t0 < c->Nt; t0 += F) {
+    for (int t0 = 0, j = 0; t0 < c->Nt; t0 += F, ++j) {
       int f = std::min(F, c->Nt - t0);
+      const int lane = lanes ? (j & 1) : 0;
+      st = lane ? side : st0;
+      T = c->d_T + lane * chunk_imgs * nvox;
       const int planes = ch * c->N[2] * f;
       if (int rc = prof_mark(c, st)) return rc;
       {
@@ -1236,6 +1258,10 @@ static int normal_op_four(Ctx* c, const SpecOps* o, const cf* X, int ns, int64_t
       if (int rc = prof_mark(c, st)) return rc;
       c->launches += 4;
     }
+  }
+  if (lanes) {   // join the side lane back into the caller's stream
+    MSLR_CUDA_TRY(cudaEventRecord(c->sn_join, side));
+    MSLR_CUDA_TRY(cudaStreamWaitEvent(st0, c->sn_join, 0));
   }
   return MSLR_OK;
 }
