@@ -178,6 +178,21 @@ int mslr_normal_op_profile(mslr_ctx* ctx, const void* X, int32_t ns_in, void* g,
 int mslr_patch_svst(mslr_ctx* ctx, int32_t scale, double beta, const void* img_in,
                     void* img_out, void* stream);
 
+/* patchSVST with one threshold per patch (src/recon.jl:263-268;
+ * src/sense_gpu.jl:153-160): `lambdas` is a host array of the scale's Np
+ * thresholds (patch order of mslr_patch_geometry), used as β of each patch.
+ * img_in may equal img_out. */
+int mslr_patch_svst_lambdas(mslr_ctx* ctx, int32_t scale, const double* lambdas, const void* img_in,
+                            void* img_out, void* stream);
+
+/* patch_nucnorm of scale `scale`'s patches of img (Nx,Ny,Nz,Nt): with
+ * lambdas == NULL Σ_patches Σσ (src/recon.jl:138-146); with a host array of
+ * Np weights, Σ_patches λ_p Σσ_p / Np (src/recon.jl:154-166).  FP64 sums in
+ * patch order; the singular values come from each patch Gram's eigenvalues.
+ * Synchronises `stream`. */
+int mslr_patch_nucnorm(mslr_ctx* ctx, int32_t scale, const double* lambdas, const void* img, double* cost,
+                       void* stream);
+
 /* The two terms of run_recon's cost (scripts/reconstruct.jl:176-194,
  * logged each iteration by its logger, :205) for X (Nx,Ny,Nz,Nt,ns_in):
  *   dc_cost  = ½ ‖A Σ_k X[..,k] − y‖²

@@ -73,6 +73,8 @@ SIGNATURES = {
     "mslr_set_wait_limit": (C.c_int, [_P, _I64]),
     "mslr_fp32_peak": (C.c_int, [C.POINTER(C.c_double), _P]),
     "mslr_pogm_step_local": (C.c_int, [_P, _P, _P, _P, _P]),
+    "mslr_patch_svst_lambdas": (C.c_int, [_P, _I32, C.POINTER(C.c_double), _P, _P, _P]),
+    "mslr_patch_nucnorm": (C.c_int, [_P, _I32, C.POINTER(C.c_double), _P, C.POINTER(C.c_double), _P]),
     "mslr_pogm_step_decide": (C.c_int, [_P, _P, _P]),
     "mslr_pogm_scalars": (C.c_int, [_P, C.POINTER(C.c_double), _P]),
     "mslr_patch_gram": (C.c_int, [_P, _I32, _P, _P, _P]),

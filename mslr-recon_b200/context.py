@@ -218,6 +218,26 @@ class MSLRContext:
                                       o.data_ptr(), _stream_ptr(stream)))
         return o
 
+    def patch_svst_lambdas(self, scale: int, lambdas, img: torch.Tensor, out=None, stream=None):
+        """patchSVST(img, λs, ...) of scale `scale` with one threshold per patch
+        (src/recon.jl:263-268)."""
+        _dev_c64(img, self.img_shape, "img")
+        lam = [float(v) for v in lambdas]
+        o = out if out is not None else torch.empty_like(img)
+        self._chk(lib.mslr_patch_svst_lambdas(self._h, int(scale), (C.c_double * len(lam))(*lam),
+                                              img.data_ptr(), o.data_ptr(), _stream_ptr(stream)))
+        return o
+
+    def patch_nucnorm(self, scale: int, img: torch.Tensor, lambdas=None, stream=None) -> float:
+        """patch_nucnorm of scale `scale`'s patches of img: Σ_p Σσ, or with
+        per-patch weights Σ_p λ_p Σσ_p / Np (src/recon.jl:138-166)."""
+        _dev_c64(img, self.img_shape, "img")
+        lam = None if lambdas is None else (C.c_double * len(lambdas))(*[float(v) for v in lambdas])
+        out = C.c_double()
+        self._chk(lib.mslr_patch_nucnorm(self._h, int(scale), lam, img.data_ptr(), C.byref(out),
+                                         _stream_ptr(stream)))
+        return float(out.value)
+
     def init_x0(self, X=None, stream=None):
         X = X if X is not None else torch.empty(self.x_shape, dtype=torch.complex64, device="cuda")
         _dev_c64(X, self.x_shape, "X")

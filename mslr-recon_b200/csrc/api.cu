@@ -70,6 +70,7 @@ static void free_ctx(mslr_ctx* c) {
   if (c->d_gbuf) cudaFree(c->d_gbuf);
   if (c->d_vjpw) cudaFree(c->d_vjpw);
   if (c->d_xsum) cudaFree(c->d_xsum);
+  if (c->d_pthr) cudaFree(c->d_pthr);
   if (c->sn_stream) cudaStreamDestroy(c->sn_stream);
   if (c->sn_fork) cudaEventDestroy(c->sn_fork);
   if (c->sn_join) cudaEventDestroy(c->sn_join);
@@ -357,6 +358,38 @@ int mslr_patch_svst(mslr_ctx* ctx, int32_t scale, double beta, const void* img_i
   CTX_RET(ctx, set_scalar(ctx->d_thr + 1, beta, st));
   CTX_RET(ctx, patch_svst(ctx, scale, ctx->d_thr + 1, 1.0, reinterpret_cast<const cf*>(img_in),
                           reinterpret_cast<cf*>(img_out), st));
+  return MSLR_OK;
+}
+
+int mslr_patch_svst_lambdas(mslr_ctx* ctx, int32_t scale, const double* lambdas, const void* img_in,
+                            void* img_out, void* stream) {
+  CTX_CHECK(ctx);
+  if (scale < 0 || scale >= ctx->Ns || !lambdas || !img_in || !img_out)
+    return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad argument"));
+  for (int64_t ip = 0; ip < ctx->scales[scale].Np; ++ip)
+    if (!(lambdas[ip] >= 0.0) || !std::isfinite(lambdas[ip]))
+      return ctx_fail(ctx, fail(MSLR_ERR_ARG, "thresholds must be finite and non-negative"));
+  CTX_RET(ctx, patch_svst_lambdas(ctx, scale, lambdas, reinterpret_cast<const cf*>(img_in),
+                                  reinterpret_cast<cf*>(img_out), reinterpret_cast<cudaStream_t>(stream)));
+  return MSLR_OK;
+}
+
+int mslr_patch_nucnorm(mslr_ctx* ctx, int32_t scale, const double* lambdas, const void* img, double* cost,
+                       void* stream) {
+  CTX_CHECK(ctx);
+  if (scale < 0 || scale >= ctx->Ns || !img || !cost) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad argument"));
+  std::vector<double> h;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  CTX_RET(ctx, patch_nucnorms(ctx, scale, reinterpret_cast<const cf*>(img), h, st));
+  CTX_RET(ctx, take_error(ctx, st));
+  double tot = 0.0;
+  if (lambdas) {   // Σ_ip λ_ip Σσ_ip / Np (src/recon.jl:154-166)
+    for (size_t ip = 0; ip < h.size(); ++ip) tot += h[ip] > 0.0 ? lambdas[ip] * h[ip] : 0.0;
+    tot /= (double)h.size();
+  } else {         // Σ_ip Σσ_ip (src/recon.jl:138-146)
+    for (double v : h) tot += v;
+  }
+  *cost = tot;
   return MSLR_OK;
 }
 

@@ -145,6 +145,7 @@ struct Ctx {
   cf* d_pbuf = nullptr;        // per-patch output buffer for non-partition scales
   size_t pbuf_elems = 0;
   cf* d_img_tmp = nullptr;     // (Nt, nvox) out-of-place staging for in-place calls
+  double* d_pthr = nullptr;    // per-patch thresholds (the largest Np of the scales)
 
   size_t bytes = 0;
   uint64_t launches = 0;   // kernels launched through this context
@@ -196,7 +197,12 @@ int svst_setup(Ctx* c);   // workspaces (create time)
 // img_out = patchSVST(img_in) for scale s with threshold (*thr_dev) * lam
 int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaStream_t st);
 int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_in, cf* img_out,
-               cudaStream_t st);
+               cudaStream_t st, int thr_per_patch = 0);
+// per-patch thresholds of a scale (patchSVST(img, λs, ...), src/recon.jl:263-268)
+int patch_svst_lambdas(Ctx* c, int s, const double* lambdas_host, const cf* img_in, cf* img_out,
+                       cudaStream_t st);
+// nuclear norms of every patch of scale s of img, in patch order (synchronises st)
+int patch_nucnorms(Ctx* c, int s, const cf* img, std::vector<double>& out, cudaStream_t st);
 int geom_build(const int N[3], int Nt, const int ps_in[3], const int ss_in[3], ScaleGeom* g);
 int geom_upload(ScaleGeom* g, const int N[3]);
 void geom_free(ScaleGeom* g);

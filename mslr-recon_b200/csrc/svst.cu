@@ -514,6 +514,11 @@ int svst_setup(Ctx* c) {
     c->pbuf_elems = pbuf;
   }
   if ((rc = dalloc(c, (void**)&c->d_img_tmp, (size_t)c->Nt * c->nvox * sizeof(cf)))) return rc;
+  {
+    int64_t npmax = 1;
+    for (auto& g : c->scales) npmax = std::max(npmax, g.Np);
+    if ((rc = dalloc(c, (void**)&c->d_pthr, (size_t)npmax * sizeof(double)))) return rc;
+  }
   int nmax = 1;
   for (auto& g : c->scales) nmax = std::max(nmax, g.n);
   if ((rc = umma_prepare())) return rc;   // before any graph capture of the iteration
@@ -521,7 +526,7 @@ int svst_setup(Ctx* c) {
 }
 
 int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_in, cf* img_out,
-               cudaStream_t st) {
+               cudaStream_t st, int thr_per_patch) {
   const ScaleGeom& g = c->scales[s];
   const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
   const int nsplit = split_of(g);
@@ -531,20 +536,67 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
   if (g.partition) {
     cf* dst = img_out;
     if (img_in == img_out) dst = c->d_img_tmp;   // Gram/rebuild read the input throughout
-    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, dst, 1, tc, ctx_wait(c), st,
+    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, thr_per_patch, lam, dst, 1, tc, ctx_wait(c), st,
                         &c->launches)))
       return rc;
     if (dst != img_out)
       MSLR_CUDA_TRY(cudaMemcpyAsync(img_out, dst, (size_t)c->Nt * c->nvox * sizeof(cf),
                                     cudaMemcpyDeviceToDevice, st));
   } else {
-    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, 0, lam, c->d_pbuf, 0, tc, ctx_wait(c), st,
-                        &c->launches)))
+    if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, thr_per_patch, lam, c->d_pbuf, 0, tc,
+                        ctx_wait(c), st, &c->launches)))
       return rc;
     k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, img_out);
     MSLR_CUDA_TRY(cudaGetLastError());
     c->launches += 1;
   }
+  return MSLR_OK;
+}
+
+int patch_svst_lambdas(Ctx* c, int s, const double* lambdas_host, const cf* img_in, cf* img_out,
+                       cudaStream_t st) {
+  const ScaleGeom& g = c->scales[s];
+  MSLR_CUDA_TRY(cudaMemcpyAsync(c->d_pthr, lambdas_host, (size_t)g.Np * sizeof(double), cudaMemcpyHostToDevice,
+                                st));
+  return patch_svst(c, s, c->d_pthr, 1.0, img_in, img_out, st, 1);
+}
+
+// Per-patch Σσ of scale s (patch_nucnorm's costs[ip], src/recon.jl:138-146):
+// Grams of every patch, then the eigen stage in values-only mode.
+int patch_nucnorms(Ctx* c, int k, const cf* X, std::vector<double>& h, cudaStream_t st) {
+  const ScaleGeom& g = c->scales[k];
+  int rc;
+  if (c->nuc_cap < g.Np) {
+    if (c->d_nuc) cudaFree(c->d_nuc);
+    c->d_nuc = nullptr;
+    c->nuc_cap = 0;
+    int64_t npmax = 0;
+    for (auto& gg : c->scales) npmax = std::max(npmax, gg.Np);
+    if ((rc = dalloc(c, (void**)&c->d_nuc, (size_t)npmax * sizeof(double)))) return rc;
+    c->nuc_cap = npmax;
+  }
+  if (!c->d_zero) {
+    if ((rc = dalloc(c, (void**)&c->d_zero, sizeof(double)))) return rc;
+    MSLR_CUDA_TRY(cudaMemsetAsync(c->d_zero, 0, sizeof(double), st));
+  }
+  const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
+  const int nsplit = choose_split(g.Np, g.n, g.L);
+  WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? k : 0].gram, g.Np, g.n, nsplit);
+  if ((rc = svst_gram(X, m, g.Np, w, nsplit, c->tc_mode(), ctx_wait(c), st, &c->launches))) return rc;
+  EigSegment seg;
+  seg.n = g.n;
+  seg.np = g.Np;
+  seg.gram = w.gram;
+  seg.zv = reinterpret_cast<cf*>(w.zv);
+  seg.aux = w.aux;
+  seg.rank = w.rank;
+  seg.lam = 0.0;
+  seg.nuc = c->d_nuc;
+  if ((rc = eig_launch_multi(1, &seg, c->d_zero, 0, st))) return rc;
+  c->launches += 1;
+  h.resize((size_t)g.Np);
+  MSLR_CUDA_TRY(cudaMemcpyAsync(h.data(), c->d_nuc, (size_t)g.Np * sizeof(double), cudaMemcpyDeviceToHost, st));
+  MSLR_CUDA_TRY(cudaStreamSynchronize(st));
   return MSLR_OK;
 }
 
@@ -850,44 +902,10 @@ int svst_batch_noalloc(int mrows, int ncols, int batch, const double* betas, con
 // in patch order in FP64.  Synchronises st.
 int patch_nucnorm_all(Ctx* c, const cf* X, double* reg_out, cudaStream_t st) {
   const int64_t E = (int64_t)c->Nt * c->nvox;
-  int64_t npmax = 0;
-  for (auto& g : c->scales) npmax = std::max(npmax, g.Np);
-  int rc;
-  if (c->nuc_cap < npmax) {
-    if (c->d_nuc) cudaFree(c->d_nuc);
-    c->d_nuc = nullptr;
-    c->nuc_cap = 0;
-    if ((rc = dalloc(c, (void**)&c->d_nuc, (size_t)npmax * sizeof(double)))) return rc;
-    c->nuc_cap = npmax;
-  }
-  if (!c->d_zero) {
-    if ((rc = dalloc(c, (void**)&c->d_zero, sizeof(double)))) return rc;
-    MSLR_CUDA_TRY(cudaMemsetAsync(c->d_zero, 0, sizeof(double), st));
-  }
-  const int tc = c->tc_mode();
   std::vector<double> h;
   double reg = 0.0;
   for (int k = 0; k < c->Ns; ++k) {
-    const ScaleGeom& g = c->scales[k];
-    const PatchMap m = map_of(g, c->N, c->Nt, c->nvox);
-    const int nsplit = choose_split(g.Np, g.n, g.L);
-    WorkPtrs w = carve(c->svw[c->svw.size() > 1 ? k : 0].gram, g.Np, g.n, nsplit);
-    if ((rc = svst_gram(X + k * E, m, g.Np, w, nsplit, tc, ctx_wait(c), st, &c->launches))) return rc;
-    EigSegment seg;
-    seg.n = g.n;
-    seg.np = g.Np;
-    seg.gram = w.gram;
-    seg.zv = reinterpret_cast<cf*>(w.zv);
-    seg.aux = w.aux;
-    seg.rank = w.rank;
-    seg.lam = 0.0;
-    seg.nuc = c->d_nuc;
-    if ((rc = eig_launch_multi(1, &seg, c->d_zero, 0, st))) return rc;
-    c->launches += 1;
-    h.resize((size_t)g.Np);
-    MSLR_CUDA_TRY(cudaMemcpyAsync(h.data(), c->d_nuc, (size_t)g.Np * sizeof(double),
-                                  cudaMemcpyDeviceToHost, st));
-    MSLR_CUDA_TRY(cudaStreamSynchronize(st));
+    if (int rc = patch_nucnorms(c, k, X + k * E, h, st)) return rc;
     double sk = 0.0;
     for (double v : h) sk += v;
     reg += c->lambdas[k] * sk;

@@ -200,6 +200,16 @@ def patch_nucnorm(P: np.ndarray) -> float:
     return total
 
 
+def patch_nucnorm_weighted(P: np.ndarray, lams) -> float:
+    """src/recon.jl:154-166: Σ over patches of λ_p · Σ svdvals (0 for a zero
+    patch), divided by the number of patches."""
+    total = 0.0
+    for ip in range(P.shape[0]):
+        s = np.linalg.svd(P[ip], compute_uv=False)
+        total += float(lams[ip]) * float(np.sum(s, dtype=np.float64)) if s[0] > 0 else 0.0
+    return total / P.shape[0]
+
+
 # ---------------------------------------------------------------------------
 # SENSE operator — src/sense_gpu.jl:51-101 (convention of MIRT.Asense with
 # fft_forward=true, unitary=true).  The adjoint is the exact adjoint of the

@@ -361,6 +361,28 @@ def test_normal_op_summed_scales(torch, M, monkeypatch, path, aligned):
         assert set(kms) == ({"pfwd", "zmask", "padj", "csum"} if path == "four" else {"zfwd", "xy", "zadj"})
 
 
+@pytest.mark.parametrize("form", ["plain", "tuned"])
+def test_per_patch_thresholds_and_nucnorm(torch, M, form):
+    """patchSVST with one λ per patch and both patch_nucnorm forms
+    (src/recon.jl:138-166, :263-268) on a grid with overlapping and clamped
+    patches, against the FP64 oracle."""
+    rng = np.random.default_rng(31)
+    N, Nt = (13, 11, 9), 20
+    ps, ss = [4, 4, 4], [3, 3, 3]
+    Nx, Ny, Nz = N
+    img = (rng.standard_normal((Nt, Nz, Ny, Nx)) + 1j * rng.standard_normal((Nt, Nz, Ny, Nx))).astype(np.complex64)
+    g = O.patch_geometry(N, ps, ss)
+    lams = rng.uniform(0.5, 6.0, g.Np)
+    with M.MSLRContext(N, 2, Nt, 10, [ps], [ss], form=form) as ctx:
+        out = ctx.patch_svst_lambdas(0, lams, dev(torch, img)).cpu().numpy()
+        ref = O.patch_svst(img.astype(np.complex128), lams, ps, ss)
+        assert rel(out, ref) < SVST_TOL[form], rel(out, ref)
+        P = O.img2patches(img.astype(np.complex128), ps, ss)
+        assert ctx.patch_nucnorm(0, dev(torch, img)) == pytest.approx(O.patch_nucnorm(P), rel=1e-5)
+        assert ctx.patch_nucnorm(0, dev(torch, img), lams) == pytest.approx(
+            O.patch_nucnorm_weighted(P, lams), rel=1e-5)
+
+
 def test_mixed_gram_sides_per_iteration(torch, M):
     """Scales whose Gram sides need both eigen variants (400 > 384 and 64) in
     one tuned-form iteration: X after every iteration within 1e-4 of the FP64

@@ -243,3 +243,15 @@ def test_large_runner_is_run_recon_arrays(synth, case):
     for a, b in zip(got, ref):
         assert O.rel_err(a, b) < 1e-12
         assert O.rel_err_chunked(a, b, chunk=777) == pytest.approx(O.rel_err(a, b), rel=1e-9, abs=1e-300)
+
+
+def test_weighted_nucnorm_matches_definition():
+    """patch_nucnorm(P, λs) (src/recon.jl:154-166): the weighted sum of the
+    patches' nuclear norms over Np; a zero patch adds nothing."""
+    rng = np.random.default_rng(12)
+    P = rng.standard_normal((4, 6, 5)) + 1j * rng.standard_normal((4, 6, 5))
+    P[2] = 0
+    lams = np.array([0.5, 2.0, 7.0, 1.5])
+    want = sum(lams[i] * np.linalg.svd(P[i], compute_uv=False).sum() for i in (0, 1, 3)) / 4
+    assert O.patch_nucnorm_weighted(P, lams) == pytest.approx(want, rel=1e-12)
+    assert O.patch_nucnorm(P) == pytest.approx(sum(np.linalg.svd(P[i], compute_uv=False).sum() for i in range(4)))
