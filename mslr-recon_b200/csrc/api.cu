@@ -5,6 +5,8 @@
 #include <string>
 
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <vector>
 #include "internal.h"
 #include "patchmap.cuh"
@@ -32,6 +34,20 @@ int dalloc(Ctx* c, void** p, size_t bytes) {
   }
   c->bytes += bytes;
   return MSLR_OK;
+}
+
+cudaError_t raise_dyn_smem(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> cur;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  int& have = cur[{dev, func}];
+  if (bytes <= have) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
 }
 
 // defined in svst.cu

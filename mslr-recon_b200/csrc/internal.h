@@ -154,6 +154,11 @@ struct Ctx {
 
 // ---- device memory helper -------------------------------------------------
 int dalloc(Ctx* c, void** p, size_t bytes);
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) that only ever raises the
+// kernel's limit on the current device: the attribute is per process, and a
+// context of a smaller shape created later must not lower the limit another
+// live context's launches rely on.  Returns the CUDA status.
+cudaError_t raise_dyn_smem(const void* func, int bytes);
 
 // ---- device-side errors (api.cu, svst.cu) -----------------------------------
 // Error word and wait limit of a context's kernels.

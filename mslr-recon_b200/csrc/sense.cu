@@ -329,9 +329,9 @@ int sense_setup_tables(Ctx* c) {
   const size_t sz = smem_z(c), sxy = smem_xy(c);
   if (sz > 227 * 1024 || sxy > 227 * 1024)
     return fail(MSLR_ERR_UNSUPPORTED, "image dimensions too large for the shared-memory FFT");
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_zadj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz));
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_xy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sxy));
+  MSLR_CUDA_TRY(raise_dyn_smem((const void*)k_zfwd, (int)sz));
+  MSLR_CUDA_TRY(raise_dyn_smem((const void*)k_zadj, (int)sz));
+  MSLR_CUDA_TRY(raise_dyn_smem((const void*)k_xy, (int)sxy));
   // frames per chunk: keep the per-coil k-space of a chunk near 0.6 GB
   const double per_frame = (double)c->Nc * c->nvox * sizeof(cf);
   int F = (int)std::max(1.0, std::floor(600e6 / per_frame));

