@@ -83,7 +83,7 @@ struct Shape {
   // four-pass form
   static constexpr size_t smem_pfwd = sizeof(cf) * (3 * (size_t)PL + ev(NX) + ev(NY)) + sizeof(uint64_t);
   static constexpr size_t smem_zmask =
-      sizeof(cf) * (2 * (size_t)S + ev(NZ)) + 4 * NZ * sizeof(uint32_t) + 2 * sizeof(uint64_t);
+      sizeof(cf) * (2 * (size_t)S + ev(NZ)) + 8 * NZ * sizeof(uint32_t) + 2 * sizeof(uint64_t);
   static constexpr size_t smem_padj = sizeof(cf) * (2 * (size_t)PL + ev(NX) + ev(NY)) + sizeof(uint64_t);
 };
 
@@ -551,8 +551,10 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
 // fastest, then frame, then y): each slab (NZ rows of NX) comes in by bulk
 // copies into one of two buffers, runs DFT_z, the mask and bDFT_z (the last
 // forward and first inverse radix passes fused around the mask), and goes back
-// by bulk copies; the other buffer's slab is in flight meanwhile.  MINB: CTAs
-// per SM the register budget is set for.
+// by bulk copies; the other buffer's slab is in flight meanwhile.  The mask
+// words of the next slab are staged (double-buffered) while the current one
+// finishes, so a unit needs one block barrier.  MINB: CTAs per SM the
+// register budget is set for.
 template <class Sh, int MINB>
 __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
     k_zmask(cf* __restrict__ T, const uint32_t* __restrict__ mask, int nwords, int t0, int nf, int ch,
@@ -563,8 +565,8 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
   extern __shared__ __align__(128) unsigned char smraw[];
   cf* SL = reinterpret_cast<cf*>(smraw);          // two slab buffers
   cf* tw = SL + 2 * S;
-  uint32_t* MB = reinterpret_cast<uint32_t*>(tw + Sh::ev(NZ));   // 4 words per kz
-  uint64_t* bar = reinterpret_cast<uint64_t*>(MB + 4 * NZ);
+  uint32_t* MB = reinterpret_cast<uint32_t*>(tw + Sh::ev(NZ));   // 2 × 4 words per kz
+  uint64_t* bar = reinterpret_cast<uint64_t*>(MB + 8 * NZ);
   const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5, lane = tid & 31;
   const int units = ch * nf * NY;
   auto slab = [&](int u) {
@@ -576,7 +578,18 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
     spec::mbar_init(&bar[1], 1);
     spec::mbar_fence_init();
   }
+  // mask words of slab u into mb: row kz spans bits [kz·PL + y·NX, + NX) of frame t0 + f
+  auto stage_mask = [&](int u, uint32_t* mb) {
+    const int r = u / ch, f = r % nf, y = r / nf;
+    const uint32_t* mrow = mask + (int64_t)(t0 + f) * nwords;
+    for (int i = tid; i < 4 * NZ; i += blockDim.x) {
+      const int kz = i >> 2;
+      const int w = (int)(((int64_t)kz * PL + (int64_t)y * NX) >> 5) + (i & 3);
+      mb[i] = (w < nwords) ? __ldg(mrow + w) : 0u;
+    }
+  };
   for (int i = tid; i < NZ; i += blockDim.x) tw[i] = twz_g[i];
+  if ((int)blockIdx.x < units) stage_mask(blockIdx.x, MB);
   __syncthreads();
   if (warp == 0) {
     for (int q = 0; q < 2; ++q) {
@@ -588,22 +601,13 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
   int k = 0;
   for (int u = blockIdx.x; u < units; u += gridDim.x, ++k) {
     const int b = k & 1;
-    const int r = u / ch, f = r % nf, y = r / nf;
-    {   // mask words of the slab: row kz spans bits [kz·PL + y·NX, + NX) of frame t0 + f
-      const uint32_t* mrow = mask + (int64_t)(t0 + f) * nwords;
-      for (int i = tid; i < 4 * NZ; i += blockDim.x) {
-        const int kz = i >> 2;
-        const int w = (int)(((int64_t)kz * PL + (int64_t)y * NX) >> 5) + (i & 3);
-        MB[i] = (w < nwords) ? __ldg(mrow + w) : 0u;
-      }
-    }
-    __syncthreads();   // mask words visible
+    const int y = (u / ch) / nf;
     if (!bad && !spec::mbar_wait(&bar[b], (unsigned)((k >> 1) & 1))) bad = true;
     cf* P = SL + b * S;
     if (!bad) {
       const cf* twc = opaque(tw);
       using Cols = SmC<1, NX>;   // line = x, element = z
-      const MaskZ<NX, PL> msk{MB, y * NX};
+      const MaskZ<NX, PL> msk{MB + b * 4 * NZ, y * NX};
 #pragma unroll 1
       for (int g = warp; g * AZ::LPW < NX; g += nw) {
         spec::wpass<NZ, AZ::R0, 1, false, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
@@ -611,8 +615,9 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
         spec::wpass<NZ, AZ::R0, AZ::R1, true, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
       }
     }
+    if (u + (int)gridDim.x < units) stage_mask(u + (int)gridDim.x, MB + (b ^ 1) * 4 * NZ);
     spec::fence_proxy_async();   // this thread's slab writes, before the bulk copies read them
-    __syncthreads();   // slab done (and the mask words free)
+    __syncthreads();   // slab done; the next slab's mask words visible
     if (warp == 0) {
       if (!bad) {
         spec::fence_proxy_async();
