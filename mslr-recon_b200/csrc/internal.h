@@ -98,8 +98,8 @@ struct Ctx {
   int spec_pfwd_ctas = 0, spec_zmask_ctas = 0, spec_padj_ctas = 0;
   bool spec_zmask1 = false;   // z-mask kernel variant with one CTA per SM
   // chunks of the four-pass form alternate between two streams ("lanes",
-  // each with its own k-space buffer) when spec_lanes == 2, so one chunk's
-  // kernels overlap the other's
+  // each with its own k-space buffer) when spec_lanes == 2 (the default;
+  // MSLR_SENSE_LANES=1 keeps one), so one chunk's kernels overlap the other's
   int spec_lanes = 1;
   cudaStream_t sn_stream = nullptr;
   cudaEvent_t sn_fork = nullptr, sn_join = nullptr;

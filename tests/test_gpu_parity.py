@@ -326,15 +326,19 @@ def test_normal_op_tensor_core_plane_pass(torch, M, monkeypatch):
     test_sense_metric_shapes(torch, M, "tuned-tc", (90, 90, 60), 18)
 
 
-@pytest.mark.parametrize("path", ["four", "three"])
+@pytest.mark.parametrize("path", ["four", "four-one-lane", "three"])
 @pytest.mark.parametrize("aligned", [True, False])
 def test_normal_op_summed_scales(torch, M, monkeypatch, path, aligned):
-    """g = A'(A Σ_k X_k − y) for two scale images at 90×90×60, 18 coils:
-    the four-pass form (summed image by k_xsum, then the four chunk kernels)
-    and the three-kernel form (MSLR_SENSE_PATH=3), with X 16-byte aligned or
-    not, against the FP64 oracle."""
+    """g = A'(A Σ_k X_k − y) for two scale images at 90×90×60, 18 coils and
+    two chunks of frames: the four-pass form (summed image by k_xsum, then
+    the four chunk kernels, chunks on two streams or, with
+    MSLR_SENSE_LANES=1, on one) and the three-kernel form
+    (MSLR_SENSE_PATH=3), with X 16-byte aligned or not, against the FP64
+    oracle."""
     if path == "three":
         monkeypatch.setenv("MSLR_SENSE_PATH", "3")
+    if path == "four-one-lane":
+        monkeypatch.setenv("MSLR_SENSE_LANES", "1")
     rng = np.random.default_rng(77)
     N, Nc, Nt = (90, 90, 60), 18, 5
     Nx, Ny, Nz = N
@@ -358,7 +362,8 @@ def test_normal_op_summed_scales(torch, M, monkeypatch, path, aligned):
         ref = O.sense_adjoint(O.sense_forward(xs, smaps, idx) - y, smaps, idx)
         assert rel(g, ref) < 1e-5, rel(g, ref)
         kms, _ = ctx.normal_profile(Xd)
-        assert set(kms) == ({"pfwd", "zmask", "padj", "csum"} if path == "four" else {"zfwd", "xy", "zadj"})
+        assert set(kms) == ({"pfwd", "zmask", "padj", "csum"} if path.startswith("four")
+                            else {"zfwd", "xy", "zadj"})
 
 
 @pytest.mark.parametrize("form", ["plain", "tuned"])
