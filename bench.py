@@ -33,10 +33,11 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = "metric"
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of
-# each kernel of the SENSE chunk (6 coils x 4 frames at 90x90x60) from an ncu
-# capture of the committed command in profiles/; ncu flushes L2 before each
-# launch, so these are cold-cache upper bounds.  Empty until captured.
-TRAFFIC_PER_LAUNCH = {}
+# each kernel of the SENSE chunk (6 coils x 4 frames at 90x90x60) from the ncu
+# capture recorded in profiles/sense_four_pass_kernels_90x90x60.md; ncu
+# flushes L2 before each launch, so these are cold-cache upper bounds (the
+# timed loop finds most of the chunk's k-space in L2).
+TRAFFIC_PER_LAUNCH = {"pfwd": 80469248, "zmask": 142843648, "padj": 164751616, "csum": 114883072}
 
 
 def describe(pb) -> str:

@@ -562,6 +562,8 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
   using AZ = typename Sh::AZ;
   constexpr int NX = Sh::NX, NY = Sh::NY, NZ = Sh::NZ, S = Sh::S, PL = Sh::PL;
   constexpr int64_t NVOX = Sh::NVOX;
+  constexpr int kGroups = Sh::cdiv(NX, AZ::LPW);   // line groups of a slab
+  constexpr bool kCopyWarp = Sh::ZW2 > 1 && kGroups % (Sh::ZW2 - 1) == 0;
   extern __shared__ __align__(128) unsigned char smraw[];
   cf* SL = reinterpret_cast<cf*>(smraw);          // two slab buffers
   cf* tw = SL + 2 * S;
@@ -608,8 +610,11 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
       const cf* twc = opaque(tw);
       using Cols = SmC<1, NX>;   // line = x, element = z
       const MaskZ<NX, PL> msk{MB + b * 4 * NZ, y * NX};
+      // when the line groups divide evenly over the other warps, warp 0 only
+      // moves slabs (its bulk stores and loads then overlap the others' passes)
+      const int cw = kCopyWarp ? 1 : 0;
 #pragma unroll 1
-      for (int g = warp; g * AZ::LPW < NX; g += nw) {
+      for (int g = warp - cw; g >= 0 && g * AZ::LPW < NX; g += nw - cw) {
         spec::wpass<NZ, AZ::R0, 1, false, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
         spec::wsandwich<NZ, AZ::R1, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P}, msk);
         spec::wpass<NZ, AZ::R0, AZ::R1, true, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
