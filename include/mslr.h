@@ -54,6 +54,14 @@ extern "C" {
 #define MSLR_FORM_TUNED 1        /* split-precision tensor-core Gram/rebuild, graph-captured iteration */
 #define MSLR_FORM_TF32 2         /* as TUNED with TF32 (not split) tensor-core Gram/rebuild products */
 
+/* pogm_mod's `mom` and `restart` options (mslr_pogm_run_options). */
+#define MSLR_MOM_PGM 0           /* :pgm  — proximal gradient */
+#define MSLR_MOM_FPGM 1          /* :fpgm — FISTA momentum */
+#define MSLR_MOM_POGM 2          /* :pogm — optimised gradient (run_recon's choice) */
+#define MSLR_RESTART_NONE 0      /* :none */
+#define MSLR_RESTART_GR 1        /* :gr — gradient restart (run_recon's choice) */
+#define MSLR_RESTART_FR 2        /* :fr — function restart on comp_cost = dc_cost + reg_cost */
+
 typedef struct mslr_ctx mslr_ctx;
 
 /* Library ABI version (MSLR_ABI_VERSION). */
@@ -224,6 +232,19 @@ int mslr_pogm_run(mslr_ctx* ctx, void* X, int32_t niter, double L, double restar
 int mslr_pogm_run_costs(mslr_ctx* ctx, void* X, int32_t niter, double L, double restart_cutoff,
                         double bsig, uint8_t* restarts_host, double* dc_costs_host,
                         double* reg_costs_host, void* stream);
+
+/* pogm_mod (src/mirt_mod.jl:74-188) with any of its options and run_recon's
+ * closures: mom (MSLR_MOM_*), restart (MSLR_RESTART_*), f_mu = mu >= 0.  For
+ * :fr, Fcost is run_recon's comp_cost (dc_cost + reg_cost, as mslr_cost).
+ * On return X holds pogm_mod's result: x_niter for :pogm, y_niter for :pgm
+ * and :fpgm.  Argument errors as src/mirt_mod.jl:88-93 (MSLR_ERR_ARG).
+ * mom = :pogm, restart = :gr, mu = 0 is mslr_pogm_run (the graph-replayed
+ * iteration); every other combination runs a host-driven loop that
+ * synchronises `stream` once or twice per iteration, and :pgm / :fpgm
+ * allocate one more (Ns, Nt, nvox) buffer on first use. */
+int mslr_pogm_run_options(mslr_ctx* ctx, void* X, int32_t niter, double L, double mu, int32_t mom,
+                          int32_t restart, double restart_cutoff, double bsig, uint8_t* restarts_host,
+                          void* stream);
 
 /* Stepwise POGM: mslr_pogm_begin sets up the state for `niter` iterations
  * from X; each mslr_pogm_step runs exactly one iteration (X holds x_i

@@ -69,6 +69,8 @@ SIGNATURES = {
     "mslr_power_iter": (C.c_int, [_P, _I32, _D, C.POINTER(C.c_double), _I32P, _P]),
     "mslr_pogm_run_costs": (C.c_int, [_P, _P, _I32, _D, _D, _D, C.POINTER(C.c_uint8),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double), _P]),
+    "mslr_pogm_run_options": (C.c_int, [_P, _P, _I32, _D, _D, _I32, _I32, _D, _D,
+                                        C.POINTER(C.c_uint8), _P]),
     "mslr_sync": (C.c_int, [_P, _P]),
     "mslr_set_wait_limit": (C.c_int, [_P, _I64]),
     "mslr_fp32_peak": (C.c_int, [C.POINTER(C.c_double), _P]),

@@ -268,6 +268,28 @@ class MSLRContext:
         self._niter = int(niter)
         return [bool(v) for v in r], [float(v) for v in dc], [float(v) for v in reg]
 
+    MOMS = {"pgm": 0, "fpgm": 1, "pogm": 2}
+    RESTARTS = {"none": 0, "gr": 1, "fr": 2}
+
+    def pogm_run_options(self, X: torch.Tensor, niter: int, L: float, mom: str = "pogm",
+                         restart: str = "gr", f_mu: float = 0.0, restart_cutoff: float = 0.0,
+                         bsig: float = 1.0, stream=None):
+        """pogm_mod with any of its options (src/mirt_mod.jl:74-188): ``mom``
+        in ("pgm", "fpgm", "pogm"), ``restart`` in ("none", "gr", "fr"),
+        ``f_mu`` >= 0.  X (x0 on entry) receives pogm_mod's result (x for
+        :pogm, y for :pgm / :fpgm).  Returns the restart flags (niter + 1)."""
+        _dev_c64(X, self.x_shape, "X")
+        if mom not in self.MOMS:
+            raise ValueError(f"mom={mom}")
+        if restart not in self.RESTARTS:
+            raise ValueError(f"restart={restart}")
+        r = (C.c_uint8 * (niter + 1))()
+        self._chk(lib.mslr_pogm_run_options(self._h, X.data_ptr(), int(niter), float(L), float(f_mu),
+                                            self.MOMS[mom], self.RESTARTS[restart], float(restart_cutoff),
+                                            float(bsig), r, _stream_ptr(stream)))
+        self._niter = int(niter)
+        return [bool(v) for v in r]
+
     def sync(self, stream=None):
         """Synchronise the stream and raise any device-side error the
         context's kernels recorded since the last check."""

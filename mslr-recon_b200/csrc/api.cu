@@ -62,7 +62,7 @@ int svst_batch_noalloc(int mrows, int ncols, int batch, const double* betas, con
 static void free_ctx(mslr_ctx* c) {
   void* ptrs[] = {c->d_tw[0], c->d_tw[1], c->d_tw[2], c->d_phase[0], c->d_phase[1], c->d_phase[2],
                   c->d_mod[0], c->d_mod[1], c->d_mod[2], c->d_smaps_mod, c->d_mask, c->d_idx,
-                  c->d_ahy, c->d_T, c->d_U, c->d_Z, c->d_G, c->d_Gold, c->d_part, c->d_state,
+                  c->d_ahy, c->d_T, c->d_U, c->d_Z, c->d_G, c->d_Gold, c->d_Y, c->d_part, c->d_state,
                   c->d_restarts, c->d_thr, c->d_err, c->d_pbuf, c->d_img_tmp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -510,6 +510,30 @@ int mslr_pogm_run_costs(mslr_ctx* ctx, void* X, int32_t niter, double L, double 
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return ctx_fail(ctx, fail(MSLR_ERR_CUDA, cudaGetErrorString(e)));
   }
+  CTX_RET(ctx, take_error(ctx, st));
+  return MSLR_OK;
+}
+
+int mslr_pogm_run_options(mslr_ctx* ctx, void* X, int32_t niter, double L, double mu, int32_t mom,
+                          int32_t restart, double restart_cutoff, double bsig, uint8_t* restarts_host,
+                          void* stream) {
+  CTX_CHECK(ctx);
+  NEED_BOUND(ctx);
+  if (!X) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "null argument"));
+  CTX_RET(ctx, check_pogm_args(ctx, niter, L, restart_cutoff, bsig));
+  // src/mirt_mod.jl:88-93
+  if (mom < MSLR_MOM_PGM || mom > MSLR_MOM_POGM) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad mom"));
+  if (restart < MSLR_RESTART_NONE || restart > MSLR_RESTART_FR)
+    return ctx_fail(ctx, fail(MSLR_ERR_ARG, "bad restart"));
+  if (!(mu >= 0.0)) return ctx_fail(ctx, fail(MSLR_ERR_ARG, "f_mu < 0"));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (mom == MSLR_MOM_POGM && restart == MSLR_RESTART_GR && mu == 0.0) {
+    // run_recon's own choice: the fused, graph-replayed iteration
+    ctx->err.clear();
+    return mslr_pogm_run(ctx, X, niter, L, restart_cutoff, bsig, restarts_host, stream);
+  }
+  CTX_RET(ctx, pogm_run_options(ctx, reinterpret_cast<cf*>(X), niter, L, mu, mom, restart,
+                                restart_cutoff, bsig, restarts_host, st));
   CTX_RET(ctx, take_error(ctx, st));
   return MSLR_OK;
 }

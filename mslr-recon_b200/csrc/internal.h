@@ -130,6 +130,7 @@ struct Ctx {
   cf* d_Z = nullptr;   // (Ns, Nt, nvox) pre-prox iterate z_i
   cf* d_G = nullptr;   // (Nt, nvox) gradient
   cf* d_Gold = nullptr;  // (Nt, nvox) previous gradient (only when bsig != 1)
+  cf* d_Y = nullptr;     // (Ns, Nt, nvox) y_i of mom = :pgm / :fpgm (allocated on first use)
   double* d_part = nullptr;   // reduction partials
   int nred_blocks = 0;
   PogmState* d_state = nullptr;
@@ -245,6 +246,8 @@ int pogm_step(Ctx* c, cf* X, cudaStream_t st);
 // totals over the ranks, the current scalars
 int pogm_step_local(Ctx* c, cf* X, cf* Zout, double* sums_dev, cudaStream_t st);
 int pogm_step_decide(Ctx* c, const double* sums_dev, cudaStream_t st);
+int pogm_run_options(Ctx* c, cf* X, int niter, double L, double mu, int mom, int restart,
+                     double cutoff, double bsig, uint8_t* restarts_h, cudaStream_t st);
 int pogm_scalars(Ctx* c, double* out, cudaStream_t st);
 int patch_gram_out(Ctx* c, int s, const cf* img, cf* gram_out, cudaStream_t st);
 int patch_svst_from_gram(Ctx* c, int s, double beta, const cf* gram, const cf* img_in, cf* img_out,

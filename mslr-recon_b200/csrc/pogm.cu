@@ -19,6 +19,8 @@
 // single pass over x, u and g; the scalar recurrence runs on the device so
 // that a whole iteration can be replayed from a CUDA graph.
 #include <cmath>
+#include <cstring>
+#include <vector>
 
 #include <string>
 
@@ -248,6 +250,59 @@ __global__ void k_scale_into(cf* __restrict__ x, const cf* __restrict__ p, float
     x[e] = cscale(p[e], s);
 }
 
+// ---- pogm_mod's other options (mom = :pgm / :fpgm, restart = :none / :fr, μ > 0) ----
+// Z[k] = X[k] − α g for every scale k (the gradient step, the same g for all)
+__global__ void k_grad_step(const cf* __restrict__ X, const cf* __restrict__ G, float alpha,
+                            cf* __restrict__ Z, int64_t E, int ns) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const cf g = G[e];
+    for (int k = 0; k < ns; ++k) {
+      const cf x = X[(int64_t)k * E + e];
+      Z[(int64_t)k * E + e] = make_float2(x.x - alpha * g.x, x.y - alpha * g.y);
+    }
+  }
+}
+
+// _gr_restart's sums for :pgm / :fpgm (src/mirt_mod.jl:26-29, :124-133):
+// Fgrad = −(ynew − xold)/α, Δy = ynew − yold; partials of Σ Re(−Fgrad·Δy),
+// ‖Fgrad‖², ‖Δy‖² over n elements (unconjugated product, FP64)
+__global__ void __launch_bounds__(kRedThreads)
+    k_pgm_sums(const cf* __restrict__ Yn, const cf* __restrict__ X, const cf* __restrict__ Yold,
+               double inv_alpha, int64_t n, double* __restrict__ part) {
+  __shared__ double sh[32];
+  double r_dot = 0.0, r_f2 = 0.0, r_d2 = 0.0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const cf yn = Yn[e], xo = X[e], yo = Yold[e];
+    const double fr = -((double)yn.x - xo.x) * inv_alpha, fi = -((double)yn.y - xo.y) * inv_alpha;
+    const double dr = (double)yn.x - yo.x, di = (double)yn.y - yo.y;
+    r_dot += -(fr * dr - fi * di);
+    r_f2 += fr * fr + fi * fi;
+    r_d2 += dr * dr + di * di;
+  }
+  double v;
+  v = block_sum(r_dot, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 4 + 0] = v;
+  v = block_sum(r_f2, sh);
+  if (threadIdx.x == 0) part[blockIdx.x * 4 + 1] = v;
+  v = block_sum(r_d2, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x * 4 + 2] = v;
+    part[blockIdx.x * 4 + 3] = 0.0;
+  }
+}
+
+// X = Yn + β (Yn − Yold) over n elements (:fpgm's momentum step)
+__global__ void k_extrapolate(cf* __restrict__ X, const cf* __restrict__ Yn, const cf* __restrict__ Yold,
+                              float beta, int64_t n) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const cf yn = Yn[e], yo = Yold[e];
+    X[e] = make_float2(yn.x + beta * (yn.x - yo.x), yn.y + beta * (yn.y - yo.y));
+  }
+}
+
 }  // namespace
 
 int set_scalar(double* dst, double v, cudaStream_t st) {
@@ -445,6 +500,173 @@ int power_iter(Ctx* c, int niter, double tol, double* sigma1, int* iters, cudaSt
   if ((rc = normal_op(c, x, 1, E, p, false, st))) return rc;
   if ((rc = dots(d))) return rc;
   *sigma1 = std::sqrt(std::max(d[0], 0.0)) / std::sqrt(d[1]);
+  return MSLR_OK;
+}
+
+}  // namespace mslr
+
+namespace mslr {
+
+// The four totals of the reduction partials in d_part, to the host.
+static int totals_to_host(Ctx* c, double* tot, double* d_tot, cudaStream_t st) {
+  k_pogm_reduce<<<1, kRedThreads, 0, st>>>(c->d_part, kRedBlocks, d_tot);
+  MSLR_CUDA_TRY(cudaGetLastError());
+  MSLR_CUDA_TRY(cudaMemcpyAsync(tot, d_tot, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  MSLR_CUDA_TRY(cudaStreamSynchronize(st));
+  c->launches += 1;
+  return MSLR_OK;
+}
+
+// g_prox of run_recon (scripts/reconstruct.jl:196-202) with threshold c·λ_k
+static int prox_all(Ctx* c, double cthr, const cf* Zin, cf* Xout, cudaStream_t st) {
+  int rc;
+  if ((rc = set_scalar(c->d_thr, cthr, st))) return rc;
+  if (c->tuned()) return patch_svst_all(c, c->d_thr, Zin, Xout, st);
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  for (int k = 0; k < c->Ns; ++k)
+    if ((rc = patch_svst(c, k, c->d_thr, c->lambdas[k], Zin + k * E, Xout + k * E, st))) return rc;
+  return MSLR_OK;
+}
+
+// run_recon's comp_cost = dc_cost + reg_cost of X (scripts/reconstruct.jl:176-194)
+static int fcost(Ctx* c, const cf* X, double* out, cudaStream_t st) {
+  double dc = 0.0, reg = 0.0;
+  int rc;
+  if ((rc = dc_cost_eval(c, X, c->Ns, &dc, st))) return rc;
+  if ((rc = patch_nucnorm_all(c, X, &reg, st))) return rc;
+  *out = dc + reg;
+  return MSLR_OK;
+}
+
+// pogm_mod (src/mirt_mod.jl:74-188) with any of its options and run_recon's
+// closures, on the host loop (one synchronisation per iteration): mom 0 =
+// :pgm, 1 = :fpgm, 2 = :pogm; restart 0 = :none, 1 = :gr, 2 = :fr; f_mu ≥ 0.
+// X holds x0 on entry and pogm_mod's return value on exit (xnew for :pogm,
+// ynew otherwise).  restarts_h (niter + 1) receives the logger's flags.
+int pogm_run_options(Ctx* c, cf* X, int niter, double L, double mu, int mom, int restart,
+                     double cutoff, double bsig, uint8_t* restarts_h, cudaStream_t st) {
+  int rc;
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  const int64_t n = (int64_t)c->Ns * E;
+  const size_t bytes = (size_t)n * sizeof(cf);
+  const double q = mu / L;
+  double* d_tot = c->d_thr + 8;   // 4 doubles of the context's scalar slots
+  std::vector<uint8_t> flags((size_t)niter + 1, 0);
+  double told = 1.0, sig = 1.0, Fcostold = 0.0;
+  if (restart == 2 && (rc = fcost(c, X, &Fcostold, st))) return rc;
+  if (mom != 2) {
+    // :pgm / :fpgm — yold in U, the prox input in Z, ynew in the second half of Z's
+    // neighbour buffer: X (xold), U (yold), Z (x − α g), Yn (ynew)
+    if (!c->d_Y && (rc = dalloc(c, (void**)&c->d_Y, bytes))) return rc;
+    cf* Yold = c->d_U;
+    cf* Yn = c->d_Y;
+    MSLR_CUDA_TRY(cudaMemcpyAsync(Yold, X, bytes, cudaMemcpyDeviceToDevice, st));
+    for (int it = 1; it <= niter; ++it) {
+      const double alpha = (mom == 0 && mu != 0.0) ? 2.0 / (L + mu) : 1.0 / L;
+      if ((rc = normal_op(c, X, c->Ns, E, c->d_G, true, st))) return rc;
+      k_grad_step<<<kRedBlocks, kRedThreads, 0, st>>>(X, c->d_G, (float)alpha, c->d_Z, E, c->Ns);
+      MSLR_CUDA_TRY(cudaGetLastError());
+      c->launches += 1;
+      if ((rc = prox_all(c, alpha, c->d_Z, Yn, st))) return rc;
+      bool rs = false;
+      if (restart != 0) {
+        if (restart == 2) {
+          double Fcostnew = 0.0;
+          if ((rc = fcost(c, Yn, &Fcostnew, st))) return rc;
+          rs = Fcostnew > Fcostold;
+          Fcostold = Fcostnew;
+        } else {
+          k_pgm_sums<<<kRedBlocks, kRedThreads, 0, st>>>(Yn, X, Yold, 1.0 / alpha, n, c->d_part);
+          MSLR_CUDA_TRY(cudaGetLastError());
+          c->launches += 1;
+          double tot[4];
+          if ((rc = totals_to_host(c, tot, d_tot, st))) return rc;
+          if (!std::isfinite(tot[0]) || !std::isfinite(tot[1]) || !std::isfinite(tot[2]))
+            return fail(MSLR_ERR_NONFINITE, "non-finite value in the restart sums");
+          rs = tot[0] <= cutoff * std::sqrt(tot[1]) * std::sqrt(tot[2]);
+        }
+        if (rs) told = 1.0;
+      }
+      flags[it] = rs ? 1 : 0;
+      double tnew = told;
+      if (mom == 1) {
+        double beta;
+        if (mu != 0.0) {
+          beta = (1.0 - std::sqrt(q)) / (1.0 + std::sqrt(q));
+        } else {
+          tnew = 0.5 * (1.0 + std::sqrt(1.0 + 4.0 * told * told));
+          beta = (told - 1.0) / tnew;
+        }
+        k_extrapolate<<<kRedBlocks, kRedThreads, 0, st>>>(X, Yn, Yold, (float)beta, n);
+        MSLR_CUDA_TRY(cudaGetLastError());
+        c->launches += 1;
+      } else {
+        MSLR_CUDA_TRY(cudaMemcpyAsync(X, Yn, bytes, cudaMemcpyDeviceToDevice, st));
+      }
+      std::swap(Yold, Yn);   // yold ← ynew
+      if (mom != 0 && mu == 0.0) told = tnew;
+    }
+    // pogm_mod returns ynew for :pgm / :fpgm
+    MSLR_CUDA_TRY(cudaMemcpyAsync(X, Yold, bytes, cudaMemcpyDeviceToDevice, st));
+  } else {
+    // :pogm with restart :none / :fr or μ > 0: the fused update of the default
+    // path with the scalars of this iteration written from the host
+    PogmState h{};
+    h.alpha = 1.0 / L;
+    h.flags = (bsig != 1.0 && restart != 0) ? 1 : 0;
+    if (h.flags) {
+      if (!c->d_Gold && (rc = dalloc(c, (void**)&c->d_Gold, (size_t)E * sizeof(cf)))) return rc;
+      MSLR_CUDA_TRY(cudaMemsetAsync(c->d_Gold, 0, (size_t)E * sizeof(cf), st));
+    }
+    MSLR_CUDA_TRY(cudaMemcpyAsync(c->d_U, X, bytes, cudaMemcpyDeviceToDevice, st));   // uold = x0
+    for (int it = 1; it <= niter; ++it) {
+      double tnew = told, beta, gamma;
+      if (mu != 0.0) {
+        const double r = 2.0 + q - std::sqrt(q * q + 8.0 * q);
+        beta = r * r / 4.0 / (1.0 - q);
+        gamma = r / 2.0;
+      } else {
+        tnew = 0.5 * (1.0 + std::sqrt(1.0 + (it == niter ? 8.0 : 4.0) * told * told));
+        beta = (told - 1.0) / tnew;
+        gamma = sig * told / tnew;
+      }
+      h.beta = beta;
+      h.gamma = gamma;
+      MSLR_CUDA_TRY(cudaMemcpyAsync(c->d_state, &h, sizeof(PogmState), cudaMemcpyHostToDevice, st));
+      if ((rc = normal_op(c, X, c->Ns, E, c->d_G, true, st))) return rc;
+      k_pogm_update<<<kRedBlocks, kRedThreads, 0, st>>>(X, c->d_U, c->d_G, c->d_Gold, c->d_Z, E, c->Ns,
+                                                        c->d_state, c->d_part);
+      MSLR_CUDA_TRY(cudaGetLastError());
+      c->launches += 1;
+      double tot[4];
+      if ((rc = totals_to_host(c, tot, d_tot, st))) return rc;
+      const double zeta = h.alpha * (1.0 + beta + gamma);
+      if ((rc = prox_all(c, zeta, c->d_Z, X, st))) return rc;
+      bool rs = false;
+      if (restart != 0) {
+        if (restart == 2) {
+          double Fcostnew = 0.0;
+          if ((rc = fcost(c, X, &Fcostnew, st))) return rc;
+          rs = Fcostnew > Fcostold;
+          Fcostold = Fcostnew;
+        } else {
+          if (!std::isfinite(tot[0]) || !std::isfinite(tot[1]) || !std::isfinite(tot[2]))
+            return fail(MSLR_ERR_NONFINITE, "non-finite value in the restart sums");
+          rs = tot[0] <= cutoff * std::sqrt((double)c->Ns * tot[1]) * std::sqrt(tot[2]);
+        }
+        if (rs) {
+          tnew = 1.0;
+          sig = 1.0;
+        } else if (h.flags && (double)c->Ns * tot[3] < 0.0) {
+          sig = bsig * sig;
+        }
+      }
+      flags[it] = rs ? 1 : 0;
+      if (mu == 0.0) told = tnew;
+    }
+  }
+  if (restarts_h) std::memcpy(restarts_h, flags.data(), flags.size());
+  MSLR_CUDA_TRY(cudaStreamSynchronize(st));
   return MSLR_OK;
 }
 

@@ -19,7 +19,7 @@ module MSLRB200
 
 using CUDA
 
-export MSLRContext, sense_forward!, sense_adjoint!, dc_cost_grad!, patch_svst!,
+export MSLRContext, pogm_mod!, sense_forward!, sense_adjoint!, dc_cost_grad!, patch_svst!,
        pogm_run!, cost, sync!, power_iter, mslr_lambdas, set_lambdas!, pogm_grad, mslr_sampling
 
 const libmslr = get(ENV, "MSLR_LIB", joinpath(@__DIR__, "..", "libmslr.so"))
@@ -174,6 +174,31 @@ function pogm_run!(ctx::MSLRContext, X::CuArray{ComplexF32}, niter::Integer, L::
                   Ptr{Cvoid}),
                  ctx.h, X, Int32(niter), Float64(L), Float64(restart_cutoff), Float64(bsig),
                  flags, _stream()), ctx.h)
+    return Bool.(flags)
+end
+
+"""
+    pogm_mod!(ctx, X, niter, L; mom=:pogm, restart=:gr, f_mu=0.0, restart_cutoff=0.0, bsig=1.0)
+
+`pogm_mod` (src/mirt_mod.jl:74-188) with any of its options and run_recon's
+closures, from `X` (x0) in place: `X` receives `xnew` for `:pogm`, `ynew` for
+`:pgm` / `:fpgm`.  `restart=:fr` uses run_recon's comp_cost.  Throws
+`ArgumentError` for an unknown `mom` / `restart`, as pogm_mod does.  Returns
+the restart flags (entry 1 is false).
+"""
+function pogm_mod!(ctx::MSLRContext, X::CuArray{ComplexF32}, niter::Integer, L::Real;
+                   mom::Symbol=:pogm, restart::Symbol=:gr, f_mu::Real=0.0,
+                   restart_cutoff::Real=0.0, bsig::Real=1.0)
+    m = Dict(:pgm => 0, :fpgm => 1, :pogm => 2)
+    r = Dict(:none => 0, :gr => 1, :fr => 2)
+    haskey(m, mom) || throw(ArgumentError("mom=$mom"))
+    haskey(r, restart) || throw(ArgumentError("restart=$restart"))
+    flags = zeros(UInt8, niter + 1)
+    _check(ccall((:mslr_pogm_run_options, libmslr), Cint,
+                 (Ptr{Cvoid}, CuPtr{ComplexF32}, Int32, Float64, Float64, Int32, Int32, Float64,
+                  Float64, Ptr{UInt8}, Ptr{Cvoid}),
+                 ctx.h, X, Int32(niter), Float64(L), Float64(f_mu), Int32(m[mom]), Int32(r[restart]),
+                 Float64(restart_cutoff), Float64(bsig), flags, _stream()), ctx.h)
     return Bool.(flags)
 end
 

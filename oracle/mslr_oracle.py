@@ -444,12 +444,16 @@ class ReconProblem:
 
 
 def run_recon_arrays(prob: ReconProblem, niters: int, dtype=np.complex128, log_costs: bool = False,
-                     iter_callback=None, restart_cutoff: float = 0.0, bsig: float = 1.0):
+                     iter_callback=None, restart_cutoff: float = 0.0, bsig: float = 1.0,
+                     mom: str = "pogm", restart: str = "gr", f_mu: float = 0.0):
     """The hot loop of scripts/reconstruct.jl:174-226 on in-memory arrays.
 
     ``dtype=np.complex128`` is the FP64 oracle; ``np.complex64`` mimics the
     reference CPU precision.  Returns (X, restarts, dc_costs, reg_costs);
-    the cost lists are empty unless ``log_costs``.
+    the cost lists are empty unless ``log_costs``.  ``mom``, ``restart`` and
+    ``f_mu`` are pogm_mod's options (run_recon passes :pogm, :gr, 0); Fcost
+    is run_recon's comp_cost = dc_cost + reg_cost, evaluated by pogm_mod
+    only where a restart rule reads it (restart = "fr").
     """
     Nx, Ny, Nz = prob.N
     Nt, Ns = prob.Nt, prob.Ns
@@ -492,7 +496,8 @@ def run_recon_arrays(prob: ReconProblem, niters: int, dtype=np.complex128, log_c
 
     X0 = np.zeros((Ns, Nt, Nz, Ny, Nx), dtype=dtype)
     X0[0] = sense_adjoint(y, smaps, idx, w)
-    Xf, _ = pogm_mod(X0, (lambda X: 0.0), dc_cost_grad, L, mom="pogm", niter=niters,
+    fcost = (lambda X: dc_cost(X) + reg_cost(X)) if restart == "fr" else (lambda X: 0.0)
+    Xf, _ = pogm_mod(X0, fcost, dc_cost_grad, L, mom=mom, restart=restart, f_mu=f_mu, niter=niters,
                      g_prox=g_prox, fun=logger, iter_callback=iter_callback,
                      restart_cutoff=restart_cutoff, bsig=bsig)
     return Xf, restarts, dcs, regs
