@@ -93,7 +93,7 @@ def test_pogm_options_match_oracle(torch, M, problem, mom, restart, f_mu, cutoff
 
 def test_pogm_options_argument_errors(torch, M, problem):
     """pogm_mod's ArgumentErrors (src/mirt_mod.jl:88-93) as MSLR_ERR_ARG."""
-    from mslr_recon_b200._lib import MSLR_ERR_ARG, MSLRError, lib
+    from mslr_recon_b200._lib import MSLR_ERR_ARG, lib
     pb = problem
     Nt, Nc, K = pb["y"].shape
     with M.MSLRContext(pb["N"], Nc, Nt, K, pb["patch_sizes"], pb["strides"]) as ctx:
@@ -111,5 +111,5 @@ def test_pogm_options_argument_errors(torch, M, problem):
                      (2, 2.0, 0.0, 2, 1, 0.0, -0.5)]:   # bsig < 0
             rc = lib.mslr_pogm_run_options(ctx._h, X.data_ptr(), *args, None, None)
             assert rc == MSLR_ERR_ARG, args
-        with pytest.raises(MSLRError):
+        with pytest.raises(ValueError):   # MSLR_ERR_ARG is raised as ValueError
             ctx.pogm_run_options(X, 2, 2.0, f_mu=-1.0)
