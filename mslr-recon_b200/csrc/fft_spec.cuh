@@ -151,8 +151,11 @@ __device__ __forceinline__ int opaque_lane() {
 
 // One radix-R pass of an axis of length N over lines [line0, line0 + LPW) ∩ [0, nl).
 // INPLACE: loads and stores address the same buffer (a __syncwarp separates them).
+// TAB: `tw` is the pass's twiddle table (build_tab), entry (r − 1)·M + j for
+// butterfly j and input r — the pass must be the second of a two-pass plan
+// (NS·R = N, so k = j); otherwise `tw` is the axis' e^{−2πik/N} array.
 // Ends with __syncwarp, so the next pass of the same lines may read the output.
-template <int N, int R, int NS, bool INV, int LPW, bool INPLACE, class Ld, class St>
+template <int N, int R, int NS, bool INV, int LPW, bool INPLACE, bool TAB = false, class Ld, class St>
 __device__ __forceinline__ void wpass(int line0, int nl, const cf* tw, const Ld& ld, const St& st) {
   constexpr int M = N / R;
   constexpr int TWS = N / (NS * R);
@@ -167,7 +170,10 @@ __device__ __forceinline__ void wpass(int line0, int nl, const cf* tw, const Ld&
   }
   const int jq = j / NS, k = j - jq * NS;
   if (act) {
-    if constexpr (NS > 1) {
+    if constexpr (TAB) {
+      static_assert(NS * R == N, "twiddle tables serve the second pass of a two-pass plan");
+      sfor<1, R>([&](auto r) { v[r] = cmul(v[r], tw_get<INV>(tw, (r - 1) * M + j)); });
+    } else if constexpr (NS > 1) {
       sfor<1, R>([&](auto r) { v[r] = cmul(v[r], tw_get<INV>(tw, r * k * TWS)); });
     }
     DK<R, INV>::run(v);
@@ -183,7 +189,8 @@ __device__ __forceinline__ void wpass(int line0, int nl, const cf* tw, const Ld&
 // Last forward pass (radix R, NS = N/R) fused with the first inverse pass
 // (radix R, NS = 1): butterfly j holds forward outputs j + r·M, exactly the
 // inverse inputs, so fn(line, e, v) runs on registers in between.
-template <int N, int R, int LPW, bool INPLACE, class Ld, class St, class Fn>
+// TAB: `tw` is the forward table of build_tab<N, R, N / R> (entry (r − 1)·M + j).
+template <int N, int R, int LPW, bool INPLACE, bool TAB = false, class Ld, class St, class Fn>
 __device__ __forceinline__ void wsandwich(int line0, int nl, const cf* tw, const Ld& ld, const St& st,
                                           const Fn& fn) {
   constexpr int M = N / R;
@@ -196,7 +203,7 @@ __device__ __forceinline__ void wsandwich(int line0, int nl, const cf* tw, const
   if (act) {
     sfor<0, R>([&](auto r) { v[r] = ld(line, j + r * M); });
     if constexpr (M > 1) {
-      sfor<1, R>([&](auto r) { v[r] = cmul(v[r], tw_get<false>(tw, r * j)); });
+      sfor<1, R>([&](auto r) { v[r] = cmul(v[r], tw_get<false>(tw, TAB ? (r - 1) * M + j : r * j)); });
     }
     DK<R, false>::run(v);
     sfor<0, R>([&](auto r) { v[r] = fn(line, j + r * M, v[r]); });
@@ -207,6 +214,22 @@ __device__ __forceinline__ void wsandwich(int line0, int nl, const cf* tw, const
     sfor<0, R>([&](auto r) { st(line, j * R + r, v[r]); });
   }
   __syncwarp();
+}
+
+// Twiddle table of the radix-R pass with M = N / R butterflies that follows a
+// pass of radix M: tab[(r − 1)·M + j] = tw[r·j] for r in [1, R), j in [0, M),
+// where tw[i] = e^{−2πi·i/N} (r·j < N, so the entries are exact copies).  In
+// a pass, the lanes of one half-warp then read consecutive entries (lanes of
+// different lines with the same j read the same one) instead of tw at
+// strides r·j, which fall on few shared-memory banks.  All threads of the
+// block take part; the caller synchronises before use.
+template <int N, int R>
+__device__ __forceinline__ void build_tab(cf* tab, const cf* __restrict__ tw) {
+  constexpr int M = N / R;
+  for (int i = threadIdx.x; i < (R - 1) * M; i += blockDim.x) {
+    const int r = i / M + 1, j = i - (r - 1) * M;
+    tab[i] = tw[r * j];
+  }
 }
 
 // ---- TMA bulk copies and mbarriers -----------------------------------------------------

@@ -80,12 +80,30 @@ struct Shape {
   static constexpr size_t smem_zadj = sizeof(cf) * (2 * (size_t)S + ev(NZ)) + sizeof(uint64_t);
   static constexpr size_t smem_xy =
       sizeof(cf) * (2 * (size_t)PL + ev(NX) + ev(NY)) + MW * sizeof(uint32_t) + sizeof(uint64_t);
-  // four-pass form
-  static constexpr size_t smem_pfwd = sizeof(cf) * (3 * (size_t)PL + ev(NX) + ev(NY)) + sizeof(uint64_t);
+  // four-pass form.  The plane kernels' work plane W (filled and read only by
+  // their own passes, never by a bulk copy) has an odd row stride PW, and the
+  // lines of a warp are spread over the plane (line l of group g is row or
+  // column g + D·l, D = n / LPW): with NX = 90 the column passes' strided
+  // accesses then fall on distinct shared-memory banks far more often than
+  // with rows of 90 complex values at neighbouring lines.
+  static constexpr int PW = NX | 1;
+  static constexpr int spread(int n, int lpw) { return (n % lpw == 0) ? n / lpw : 0; }
+  static constexpr int DC = spread(NX, AY::LPW);   // column lines (x) of the plane passes
+  static constexpr int DR = spread(NY, AX::LPW);   // row lines (y)
+  static constexpr size_t smem_pfwd =
+      sizeof(cf) * (2 * (size_t)PL + (size_t)PW * NY + ev(NX) + ev(NY)) + sizeof(uint64_t);
   static constexpr size_t smem_zmask =
-      sizeof(cf) * (2 * (size_t)S + ev(NZ)) + 8 * NZ * sizeof(uint32_t) + 2 * sizeof(uint64_t);
-  static constexpr size_t smem_padj = sizeof(cf) * (2 * (size_t)PL + ev(NX) + ev(NY)) + sizeof(uint64_t);
+      sizeof(cf) * (2 * (size_t)S + 2 * ev(NZ)) + 8 * NZ * sizeof(uint32_t) + 2 * sizeof(uint64_t);
+  static constexpr size_t smem_padj =
+      sizeof(cf) * ((size_t)PL + (size_t)PW * NY + ev(NX) + ev(NY)) + sizeof(uint64_t);
 };
+
+// line l of a warp's group → row / column index (identity when D == 0)
+template <int LPW, int D>
+__device__ __forceinline__ int line_at(int l) {
+  if constexpr (D > 0) return (l / LPW) + D * (l % LPW);
+  return l;
+}
 
 // xs[z][x] · S'_c[z][x], both in shared memory (line = x, element = z)
 template <int NX>
@@ -419,22 +437,30 @@ __global__ void k_xsum(const cf* __restrict__ X, int ns, int64_t sstride, cf* __
   }
 }
 
-// a[i] · b[i], both in shared memory (line l, element e at l·SL + e·SE)
-template <int SL, int SE>
+// a[i] · b[i], both in shared memory (line l, element e at line_at(l)·SL + e·SE)
+template <int SL, int SE, int LPW = 1, int D = 0>
 struct LdMul {
   const cf* a;
   const cf* b;
   __device__ __forceinline__ cf operator()(int l, int e) const {
-    return cmul(a[l * SL + e * SE], b[l * SL + e * SE]);
+    const int i = line_at<LPW, D>(l) * SL + e * SE;
+    return cmul(a[i], b[i]);
   }
 };
-// dst[i] = conj(s[i]) · v, row layout (line = row, element = x); s in global memory
-template <int NX>
+// element e of line l at b[line_at(l)·SL + e·SE]
+template <int SL, int SE, int LPW, int D>
+struct SmM {
+  cf* b;
+  __device__ __forceinline__ cf operator()(int l, int e) const { return b[line_at<LPW, D>(l) * SL + e * SE]; }
+  __device__ __forceinline__ void operator()(int l, int e, cf v) const { b[line_at<LPW, D>(l) * SL + e * SE] = v; }
+};
+// dst[i] = conj(s[i]) · v, row layout (line = row line_at(l), element = x); s in global memory
+template <int NX, int LPW = 1, int D = 0>
 struct StMulC {
   cf* dst;
   const cf* s;
   __device__ __forceinline__ void operator()(int l, int e, cf v) const {
-    const int i = l * NX + e;
+    const int i = line_at<LPW, D>(l) * NX + e;
     dst[i] = cmulc(__ldg(s + i), v);
   }
 };
@@ -451,37 +477,40 @@ struct MaskZ {
 };
 
 // Pass groups of the plane kernels, out of line (each keeps its own index
-// arithmetic, within the 128-register budget of 16 warps).
+// arithmetic, within the 128-register budget of 16 warps).  The second pass
+// of each axis reads its twiddles from a table (build_tab); W has row stride
+// Sh::PW and the lines of a group are spread (Sh::DC, Sh::DR).
 template <class Sh>
-__device__ __noinline__ void pf_cols(const cf* xs, const cf* sc, cf* W, const cf* twy, int l0) {
+__device__ __noinline__ void pf_cols(const cf* xs, const cf* sc, cf* W, const cf* tby, int l0) {
   using AY = typename Sh::AY;
-  using Cols = SmC<1, Sh::NX>;
-  spec::wpass<Sh::NY, AY::R0, 1, false, AY::LPW, false>(l0, Sh::NX, twy, LdMul<1, Sh::NX>{xs, sc},
-                                                        Cols{W});
-  spec::wpass<Sh::NY, AY::R1, AY::R0, false, AY::LPW, true>(l0, Sh::NX, twy, Cols{W}, Cols{W});
+  using Cols = SmM<1, Sh::PW, AY::LPW, Sh::DC>;
+  spec::wpass<Sh::NY, AY::R0, 1, false, AY::LPW, false>(
+      l0, Sh::NX, tby, LdMul<1, Sh::NX, AY::LPW, Sh::DC>{xs, sc}, Cols{W});
+  spec::wpass<Sh::NY, AY::R1, AY::R0, false, AY::LPW, true, true>(l0, Sh::NX, tby, Cols{W}, Cols{W});
 }
 template <class Sh>
-__device__ __noinline__ void pf_rows(cf* W, const cf* twx, int l0, cf* dst) {
+__device__ __noinline__ void pf_rows(cf* W, const cf* tbx, int l0, cf* dst) {
   using AX = typename Sh::AX;
-  using Rows = SmC<Sh::NX, 1>;
-  spec::wpass<Sh::NX, AX::R0, 1, false, AX::LPW, true>(l0, Sh::NY, twx, Rows{W}, Rows{W});
-  spec::wpass<Sh::NX, AX::R1, AX::R0, false, AX::LPW, false>(l0, Sh::NY, twx, Rows{W}, Rows{dst});
+  using Rows = SmM<Sh::PW, 1, AX::LPW, Sh::DR>;
+  using Out = SmM<Sh::NX, 1, AX::LPW, Sh::DR>;
+  spec::wpass<Sh::NX, AX::R0, 1, false, AX::LPW, true>(l0, Sh::NY, tbx, Rows{W}, Rows{W});
+  spec::wpass<Sh::NX, AX::R1, AX::R0, false, AX::LPW, false, true>(l0, Sh::NY, tbx, Rows{W}, Out{dst});
 }
 template <class Sh>
-__device__ __noinline__ void pa_cols(const cf* P, cf* W, const cf* twy, int l0) {
+__device__ __noinline__ void pa_cols(const cf* P, cf* W, const cf* tby, int l0) {
   using AY = typename Sh::AY;
-  using Cols = SmC<1, Sh::NX>;
-  spec::wpass<Sh::NY, AY::R1, 1, true, AY::LPW, false>(l0, Sh::NX, twy, Cols{const_cast<cf*>(P)},
-                                                       Cols{W});
-  spec::wpass<Sh::NY, AY::R0, AY::R1, true, AY::LPW, true>(l0, Sh::NX, twy, Cols{W}, Cols{W});
+  using In = SmM<1, Sh::NX, AY::LPW, Sh::DC>;
+  using Cols = SmM<1, Sh::PW, AY::LPW, Sh::DC>;
+  spec::wpass<Sh::NY, AY::R1, 1, true, AY::LPW, false>(l0, Sh::NX, tby, In{const_cast<cf*>(P)}, Cols{W});
+  spec::wpass<Sh::NY, AY::R0, AY::R1, true, AY::LPW, true, true>(l0, Sh::NX, tby, Cols{W}, Cols{W});
 }
 template <class Sh>
-__device__ __noinline__ void pa_rows(cf* W, const cf* twx, int l0, cf* dst, const cf* sc) {
+__device__ __noinline__ void pa_rows(cf* W, const cf* tbx, int l0, cf* dst, const cf* sc) {
   using AX = typename Sh::AX;
-  using Rows = SmC<Sh::NX, 1>;
-  spec::wpass<Sh::NX, AX::R1, 1, true, AX::LPW, true>(l0, Sh::NY, twx, Rows{W}, Rows{W});
-  spec::wpass<Sh::NX, AX::R0, AX::R1, true, AX::LPW, false>(l0, Sh::NY, twx, Rows{W},
-                                                            StMulC<Sh::NX>{dst, sc});
+  using Rows = SmM<Sh::PW, 1, AX::LPW, Sh::DR>;
+  spec::wpass<Sh::NX, AX::R1, 1, true, AX::LPW, true>(l0, Sh::NY, tbx, Rows{W}, Rows{W});
+  spec::wpass<Sh::NX, AX::R0, AX::R1, true, AX::LPW, false, true>(
+      l0, Sh::NY, tbx, Rows{W}, StMulC<Sh::NX, AX::LPW, Sh::DR>{dst, sc});
 }
 
 // Forward plane pass of one coil group, persistent over units u = (cc
@@ -500,10 +529,10 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
   extern __shared__ __align__(128) unsigned char smraw[];
   cf* XS = reinterpret_cast<cf*>(smraw);
   cf* SB = XS + PL;
-  cf* W = SB + PL;
-  cf* twx = W + PL;
-  cf* twy = twx + Sh::ev(NX);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(twy + Sh::ev(NY));
+  cf* W = SB + PL;                  // row stride Sh::PW
+  cf* tbx = W + Sh::PW * NY;        // twiddle tables of the second x and y passes
+  cf* tby = tbx + Sh::ev(NX);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tby + Sh::ev(NY));
   const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
   const int units = ch * NZ * nf;
   auto issue = [&](int u) {
@@ -516,8 +545,8 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
     spec::mbar_init(bar, 1);
     spec::mbar_fence_init();
   }
-  for (int i = tid; i < NX; i += blockDim.x) twx[i] = twx_g[i];
-  for (int i = tid; i < NY; i += blockDim.x) twy[i] = twy_g[i];
+  spec::build_tab<NX, AX::R1>(tbx, twx_g);
+  spec::build_tab<NY, AY::R1>(tby, twy_g);
   __syncthreads();
   int u = blockIdx.x;
   if (tid == 0 && u < units) issue(u);
@@ -528,7 +557,7 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
     par ^= 1u;
     if (!bad) {
 #pragma unroll 1
-      for (int g = warp; g * AY::LPW < NX; g += nw) pf_cols<Sh>(XS, SB, W, twy, g * AY::LPW);
+      for (int g = warp; g * AY::LPW < NX; g += nw) pf_cols<Sh>(XS, SB, W, tby, g * AY::LPW);
     }
     __syncthreads();   // columns done: XS, SB free
     const int nxt = u + (int)gridDim.x;
@@ -540,7 +569,7 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
       const int cc = u % ch, r = u / ch, z = r % NZ, f = r / NZ;
       cf* dst = T + ((int64_t)f * ch + cc) * NVOX + (int64_t)z * PL;
 #pragma unroll 1
-      for (int g = warp; g * AX::LPW < NY; g += nw) pf_rows<Sh>(W, twx, g * AX::LPW, dst);
+      for (int g = warp; g * AX::LPW < NY; g += nw) pf_rows<Sh>(W, tbx, g * AX::LPW, dst);
     }
     __syncthreads();   // rows done: W free
   }
@@ -566,8 +595,9 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
   constexpr bool kCopyWarp = Sh::ZW2 > 1 && kGroups % (Sh::ZW2 - 1) == 0;
   extern __shared__ __align__(128) unsigned char smraw[];
   cf* SL = reinterpret_cast<cf*>(smraw);          // two slab buffers
-  cf* tw = SL + 2 * S;
-  uint32_t* MB = reinterpret_cast<uint32_t*>(tw + Sh::ev(NZ));   // 2 × 4 words per kz
+  cf* tf = SL + 2 * S;                            // twiddle tables: forward (the fused pass)
+  cf* ti = tf + Sh::ev(NZ);                       // and inverse (the last pass)
+  uint32_t* MB = reinterpret_cast<uint32_t*>(ti + Sh::ev(NZ));   // 2 × 4 words per kz
   uint64_t* bar = reinterpret_cast<uint64_t*>(MB + 8 * NZ);
   const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5, lane = tid & 31;
   const int units = ch * nf * NY;
@@ -590,7 +620,8 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
       mb[i] = (w < nwords) ? __ldg(mrow + w) : 0u;
     }
   };
-  for (int i = tid; i < NZ; i += blockDim.x) tw[i] = twz_g[i];
+  spec::build_tab<NZ, AZ::R1>(tf, twz_g);
+  spec::build_tab<NZ, AZ::R0>(ti, twz_g);
   if ((int)blockIdx.x < units) stage_mask(blockIdx.x, MB);
   __syncthreads();
   if (warp == 0) {
@@ -607,7 +638,8 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
     if (!bad && !spec::mbar_wait(&bar[b], (unsigned)((k >> 1) & 1))) bad = true;
     cf* P = SL + b * S;
     if (!bad) {
-      const cf* twc = opaque(tw);
+      const cf* tfc = opaque(tf);
+      const cf* tic = opaque(ti);
       using Cols = SmC<1, NX>;   // line = x, element = z
       const MaskZ<NX, PL> msk{MB + b * 4 * NZ, y * NX};
       // when the line groups divide evenly over the other warps, warp 0 only
@@ -615,9 +647,9 @@ __global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
       const int cw = kCopyWarp ? 1 : 0;
 #pragma unroll 1
       for (int g = warp - cw; g >= 0 && g * AZ::LPW < NX; g += nw - cw) {
-        spec::wpass<NZ, AZ::R0, 1, false, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
-        spec::wsandwich<NZ, AZ::R1, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P}, msk);
-        spec::wpass<NZ, AZ::R0, AZ::R1, true, AZ::LPW, true>(g * AZ::LPW, NX, twc, Cols{P}, Cols{P});
+        spec::wpass<NZ, AZ::R0, 1, false, AZ::LPW, true>(g * AZ::LPW, NX, tfc, Cols{P}, Cols{P});
+        spec::wsandwich<NZ, AZ::R1, AZ::LPW, true, true>(g * AZ::LPW, NX, tfc, Cols{P}, Cols{P}, msk);
+        spec::wpass<NZ, AZ::R0, AZ::R1, true, AZ::LPW, true, true>(g * AZ::LPW, NX, tic, Cols{P}, Cols{P});
       }
     }
     if (u + (int)gridDim.x < units) stage_mask(u + (int)gridDim.x, MB + (b ^ 1) * 4 * NZ);
@@ -656,10 +688,10 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
   constexpr int64_t NVOX = Sh::NVOX;
   extern __shared__ __align__(128) unsigned char smraw[];
   cf* P = reinterpret_cast<cf*>(smraw);
-  cf* W = P + PL;
-  cf* twx = W + PL;
-  cf* twy = twx + Sh::ev(NX);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(twy + Sh::ev(NY));
+  cf* W = P + PL;                   // row stride Sh::PW
+  cf* tbx = W + Sh::PW * NY;        // twiddle tables of the second x and y inverse passes
+  cf* tby = tbx + Sh::ev(NX);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tby + Sh::ev(NY));
   const int tid = threadIdx.x, warp = tid >> 5, nw = blockDim.x >> 5;
   const int units = ch * NZ * nf;
   auto plane = [&](int u) {
@@ -670,8 +702,8 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
     spec::mbar_init(bar, 1);
     spec::mbar_fence_init();
   }
-  for (int i = tid; i < NX; i += blockDim.x) twx[i] = twx_g[i];
-  for (int i = tid; i < NY; i += blockDim.x) twy[i] = twy_g[i];
+  spec::build_tab<NX, AX::R0>(tbx, twx_g);
+  spec::build_tab<NY, AY::R0>(tby, twy_g);
   __syncthreads();
   int u = blockIdx.x;
   if (tid == 0 && u < units) {
@@ -685,7 +717,7 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
     par ^= 1u;
     if (!bad) {
 #pragma unroll 1
-      for (int g = warp; g * AY::LPW < NX; g += nw) pa_cols<Sh>(P, W, twy, g * AY::LPW);
+      for (int g = warp; g * AY::LPW < NX; g += nw) pa_cols<Sh>(P, W, tby, g * AY::LPW);
     }
     __syncthreads();   // columns done: P free
     const int nxt = u + (int)gridDim.x;
@@ -699,7 +731,7 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
       const cf* sc = smod + (int64_t)(cc0 + cc) * NVOX + (int64_t)z * PL;
       cf* dst = plane(u);
 #pragma unroll 1
-      for (int g = warp; g * AX::LPW < NY; g += nw) pa_rows<Sh>(W, twx, g * AX::LPW, dst, sc);
+      for (int g = warp; g * AX::LPW < NY; g += nw) pa_rows<Sh>(W, tbx, g * AX::LPW, dst, sc);
     }
     __syncthreads();   // rows done: W free
   }
