@@ -142,14 +142,14 @@ size_t part_bytes(int n) {
 
 size_t vec_bytes(int n) {
   const size_t np = (size_t)n + 32;
-  return 3 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) + 3 * (size_t)n * sizeof(float) +
-         64 * sizeof(float) + 64 * sizeof(double);
+  return np * sizeof(float4) + 4 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
+         3 * (size_t)n * sizeof(float) + 64 * sizeof(float) + 64 * sizeof(double);
 }
 
 // Buffers of the back-transform besides the vector stage: Y (n × kNb), T and
 // YᴴY (kNb × kNb each), S and T·S (kNb × kCW each), one partial sum per thread.
 size_t wy_bytes(int n, int threads) {
-  return ((size_t)n * kNb + 2 * kNb * kNb + 2 * kNb * kCW + (size_t)threads) * sizeof(cf);
+  return ((size_t)n * kNb + 2 * kNb * kNb + 2 * kNb * kCW + (size_t)threads + 1) * sizeof(cf);
 }
 
 // The region after the vectors, by phase: the matvec partial sums (phase 1,
@@ -175,6 +175,167 @@ int stage_cols(int n, int threads) {
   return rz;
 }
 
+// Eight columns of a tile row: the pending rank-2 update of element
+// (row, jb + b), its contribution to the row sum y_row and to the column
+// partials (cr, ci), written back.
+__device__ __forceinline__ void tile_group(cf* a, const float4* pw, const float4* vv, cf vpr, cf wpr, cf vr,
+                                           float& yr, float& yim, float* cr, float* ci) {
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const float4 p = pw[b];   // (vp_j, wp_j)
+    const float4 v2 = vv[b >> 1];
+    const float vjx = (b & 1) ? v2.z : v2.x, vjy = (b & 1) ? v2.w : v2.y;
+    cf e = a[b];
+    e.x -= (vpr.x * p.z + vpr.y * p.w) + (wpr.x * p.x + wpr.y * p.y);
+    e.y -= (vpr.y * p.z - vpr.x * p.w) + (wpr.y * p.x - wpr.x * p.y);
+    a[b] = e;
+    yr += e.x * vjx - e.y * vjy;
+    yim += e.x * vjy + e.y * vjx;
+    cr[b] = e.x * vr.x + e.y * vr.y;
+    ci[b] = e.x * vr.y - e.y * vr.x;
+  }
+}
+
+// Column sums of eight columns over the 32 lanes (a shuffle transpose): lane l
+// ends with the sum of column l / 4 in cr[0], ci[0].
+__device__ __forceinline__ void col_sums(float* cr, float* ci, int lane) {
+  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float sr_ = h16 ? cr[q] : cr[q + 4], si_ = h16 ? ci[q] : ci[q + 4];
+    const float kr = h16 ? cr[q + 4] : cr[q], ki = h16 ? ci[q + 4] : ci[q];
+    cr[q] = kr + __shfl_xor_sync(0xffffffffu, sr_, 16);
+    ci[q] = ki + __shfl_xor_sync(0xffffffffu, si_, 16);
+  }
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const float sr_ = h8 ? cr[q] : cr[q + 2], si_ = h8 ? ci[q] : ci[q + 2];
+    const float kr = h8 ? cr[q + 2] : cr[q], ki = h8 ? ci[q + 2] : ci[q];
+    cr[q] = kr + __shfl_xor_sync(0xffffffffu, sr_, 8);
+    ci[q] = ki + __shfl_xor_sync(0xffffffffu, si_, 8);
+  }
+  {
+    const float sr_ = h4 ? cr[0] : cr[1], si_ = h4 ? ci[0] : ci[1];
+    const float kr = h4 ? cr[1] : cr[0], ki = h4 ? ci[1] : ci[0];
+    cr[0] = kr + __shfl_xor_sync(0xffffffffu, sr_, 4);
+    ci[0] = ki + __shfl_xor_sync(0xffffffffu, si_, 4);
+  }
+  cr[0] += __shfl_xor_sync(0xffffffffu, cr[0], 2);
+  ci[0] += __shfl_xor_sync(0xffffffffu, ci[0], 2);
+  cr[0] += __shfl_xor_sync(0xffffffffu, cr[0], 1);
+  ci[0] += __shfl_xor_sync(0xffffffffu, ci[0], 1);
+}
+
+// A tile (I, J), J < I, whose 32 rows and 32 columns all lie inside the
+// matrix: the same arithmetic as the general tile path without its
+// per-element tests; the column values come from the re-based vectors as
+// 16-byte loads, and each group's loads are issued before the previous
+// group is updated and stored (they address other columns) when PIPE (the
+// 384-thread variant; the 1024-thread variant's 64 registers do not hold
+// the second group).
+template <bool PIPE>
+__device__ __noinline__ void full_tile(cf* A, int n, int o, int I, int J, int t, int lane, const float4* spw,
+                                       const cf* svr, const cf* svp, const cf* swp, const cf* sv, cf* part) {
+  const int row = o + I * 32 + lane;
+  const cf vpr = svp[row], wpr = swp[row], vr = sv[row];
+  float yr = 0.f, yim = 0.f;
+  const int jo = J * 32;   // first column − o
+  cf* col0 = A + (int64_t)(o + jo) * n + row;
+  const float4* pw = spw + jo;
+  const float4* vv = reinterpret_cast<const float4*>(svr + jo);
+  cf a[8];
+  if constexpr (PIPE) {
+#pragma unroll
+    for (int b = 0; b < 8; ++b) a[b] = __ldcg(col0 + (int64_t)b * n);
+  }
+#pragma unroll 1
+  for (int g8 = 0; g8 < 4; ++g8) {
+    cf nx[8];
+    if constexpr (PIPE) {
+      if (g8 < 3) {
+#pragma unroll
+        for (int b = 0; b < 8; ++b) nx[b] = __ldcg(col0 + (int64_t)((g8 + 1) * 8 + b) * n);
+      }
+    } else {
+#pragma unroll
+      for (int b = 0; b < 8; ++b) a[b] = __ldcg(col0 + (int64_t)(g8 * 8 + b) * n);
+    }
+    float cr[8], ci[8];
+    tile_group(a, pw + g8 * 8, vv + g8 * 4, vpr, wpr, vr, yr, yim, cr, ci);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) col0[(int64_t)(g8 * 8 + b) * n] = a[b];
+    col_sums(cr, ci, lane);
+    if ((lane & 3) == 0) part[(2 * t + 1) * 32 + g8 * 8 + (lane >> 2)] = make_float2(cr[0], ci[0]);
+    if constexpr (PIPE) {
+#pragma unroll
+      for (int b = 0; b < 8; ++b) a[b] = nx[b];
+    }
+  }
+  part[2 * t * 32 + lane] = make_float2(yr, yim);
+}
+
+// One eigenvector in global memory (column `col` of Z, row stride n) through
+// one WY block of kNb reflectors starting at row k0 + 1: S = Yᴴ z, S ← T S,
+// z −= Y S.  Y's rows are read as 16-byte pairs (sYb is 16-byte aligned) and
+// the vector's elements kB rows ahead of their use.
+__device__ __noinline__ void bt_vector(cf* Z, int n, int col, int k0, const cf* sYb, const cf* sT) {
+  cf Sv[kNb];
+#pragma unroll
+  for (int jj = 0; jj < kNb; ++jj) Sv[jj] = make_float2(0.f, 0.f);
+  constexpr int kB = 4;
+  auto accum = [&](int row, const cf z) {
+    const float4* y4 = reinterpret_cast<const float4*>(sYb + row * kNb);
+#pragma unroll
+    for (int q = 0; q < kNb / 2; ++q) {
+      const float4 yy = y4[q];
+      Sv[2 * q].x += yy.x * z.x + yy.y * z.y;
+      Sv[2 * q].y += yy.x * z.y - yy.y * z.x;
+      Sv[2 * q + 1].x += yy.z * z.x + yy.w * z.y;
+      Sv[2 * q + 1].y += yy.z * z.y - yy.w * z.x;
+    }
+  };
+  {
+    int row = k0 + 1;
+    for (; row + kB <= n; row += kB) {
+      cf z[kB];
+#pragma unroll
+      for (int b = 0; b < kB; ++b) z[b] = __ldcg(Z + (int64_t)(row + b) * n + col);
+#pragma unroll
+      for (int b = 0; b < kB; ++b) accum(row + b, z[b]);
+    }
+    for (; row < n; ++row) accum(row, __ldcg(Z + (int64_t)row * n + col));
+  }
+  // T upper-triangular: S[a] is last needed by row a itself (in place)
+#pragma unroll
+  for (int a = 0; a < kNb; ++a) {
+    cf sacc = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int b = a; b < kNb; ++b) sacc = cadd(sacc, cmul(sT[a * kNb + b], Sv[b]));
+    Sv[a] = sacc;
+  }
+  auto upd = [&](int row, cf z) {
+    const float4* y4 = reinterpret_cast<const float4*>(sYb + row * kNb);
+#pragma unroll
+    for (int q = 0; q < kNb / 2; ++q) {
+      const float4 yy = y4[q];
+      z = csub(z, cmul(make_float2(yy.x, yy.y), Sv[2 * q]));
+      z = csub(z, cmul(make_float2(yy.z, yy.w), Sv[2 * q + 1]));
+    }
+    return z;
+  };
+  int row = k0 + 1;
+  for (; row + kB <= n; row += kB) {
+    cf z[kB];
+#pragma unroll
+    for (int b = 0; b < kB; ++b) z[b] = __ldcg(Z + (int64_t)(row + b) * n + col);
+#pragma unroll
+    for (int b = 0; b < kB; ++b) z[b] = upd(row + b, z[b]);
+#pragma unroll
+    for (int b = 0; b < kB; ++b) Z[(int64_t)(row + b) * n + col] = z[b];
+  }
+  for (; row < n; ++row) Z[(int64_t)row * n + col] = upd(row, Z[(int64_t)row * n + col]);
+}
+
 template <int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -196,7 +357,12 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   double* ee2 = ee + n;                             // e²              [n]
   double* lam = ee2 + n;                            // eigenvalues     [n]
   double* redd = lam + n;                           // 64 doubles
-  cf* sv = reinterpret_cast<cf*>(redd + 64);        // v of this step  [npad]
+  // the step's vectors again, indexed from the trailing block's first row o =
+  // k + 1 (16-byte aligned, so a tile's eight columns load as vectors):
+  // spw[j − o] = (vp_j, wp_j), svr[j − o] = v_j
+  float4* spw = reinterpret_cast<float4*>(redd + 64);   //             [npad]
+  cf* svr = reinterpret_cast<cf*>(spw + npad);           //             [npad]
+  cf* sv = svr + npad;                              // v of this step  [npad]
   cf* svp = sv + npad;                              // previous v      [npad]
   cf* swp = svp + npad;                             // previous w      [npad]
   float* hv = reinterpret_cast<float*>(swp + npad); // h               [n]
@@ -219,6 +385,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     sv[q] = make_float2(0.f, 0.f);
     svp[q] = make_float2(0.f, 0.f);
     swp[q] = make_float2(0.f, 0.f);
+    svr[q] = make_float2(0.f, 0.f);
+    spw[q] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
   const int i = tid;   // row owned by this thread (n <= kT)
@@ -281,6 +449,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
       A[(int64_t)k * n + i] = vi;   // reflector kept below the subdiagonal
     }
     if (i < n) sv[i] = vi;
+    if (i > k && i < n) svr[i - k - 1] = vi;
     __syncthreads();
     // fused over the trailing lower triangle [o, n)²: A22 ← A22 − (vp wpᴴ + wp vpᴴ)
     // and y = A22 v (Hermitian: element (r, c), r > c, also gives y_c += conj(a) v_r).
@@ -293,6 +462,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
         while ((I + 1) * (I + 2) / 2 <= t) ++I;
         while (I * (I + 1) / 2 > t) --I;
         const int J = t - I * (I + 1) / 2;
+        if (I != J && o + I * 32 + 32 <= n) {
+          full_tile<(MAXT <= kSmallT)>(A, n, o, I, J, t, lane, spw, svr, svp, swp, sv, part);
+          continue;
+        }
         const bool diag = (I == J);
         const int row = o + I * 32 + lane;
         const bool rowok = row < n;
@@ -397,6 +570,10 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
       }
       swp[i] = w;
       svp[i] = refl ? vi : make_float2(0.f, 0.f);
+      if (i > k + 1) {
+        const cf vq = refl ? vi : make_float2(0.f, 0.f);
+        spw[i - k - 2] = make_float4(vq.x, vq.y, w.x, w.y);
+      }
     }
     __syncthreads();
   }
@@ -651,7 +828,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   // (row, vector) element, in passes of kCW vectors.  Vectors in global
   // memory (many): thread i updates vector i with its block coefficients in
   // registers.
-  cf* sYb = sY + (int64_t)n * g.rz;   // Y: n × kNb, [row][reflector], after the vector stage
+  // Y: n × kNb, [row][reflector], after the vector stage (16-byte aligned)
+  cf* sYb = sY + (((int64_t)n * g.rz + 1) & ~(int64_t)1);
   cf* sT = sYb + (int64_t)n * kNb;    // kNb × kNb, T[a][b] at a*kNb + b
   cf* sYY = sT + kNb * kNb;           // Yᴴ Y
   cf* sS = sYY + kNb * kNb;           // kNb × kCW
@@ -700,48 +878,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     }
     __syncthreads();
     if (!stg) {   // vectors in global memory: thread tid updates vector tid (S = Yᴴ z; S ← T S; z −= Y S)
-      if (tid < r) {
-        cf Sv[kNb];
-#pragma unroll
-        for (int jj = 0; jj < kNb; ++jj) Sv[jj] = make_float2(0.f, 0.f);
-        for (int row = k0 + 1; row < n; ++row) {
-          const cf z = Z[(int64_t)row * n + tid];
-#pragma unroll
-          for (int jj = 0; jj < kNb; ++jj) {
-            const cf y = sYb[row * kNb + jj];   // conj(y)·z
-            Sv[jj].x += y.x * z.x + y.y * z.y;
-            Sv[jj].y += y.x * z.y - y.y * z.x;
-          }
-        }
-        // T upper-triangular: S[a] is last needed by row a itself (in place)
-#pragma unroll
-        for (int a = 0; a < kNb; ++a) {
-          cf sacc = make_float2(0.f, 0.f);
-#pragma unroll
-          for (int b = a; b < kNb; ++b) sacc = cadd(sacc, cmul(sT[a * kNb + b], Sv[b]));
-          Sv[a] = sacc;
-        }
-        constexpr int kB = 8;   // rows per batch: loads issued before stores
-        int row = k0 + 1;
-        for (; row + kB <= n; row += kB) {
-          cf z[kB];
-#pragma unroll
-          for (int b = 0; b < kB; ++b) z[b] = __ldcg(Z + (int64_t)(row + b) * n + tid);
-#pragma unroll
-          for (int b = 0; b < kB; ++b) {
-#pragma unroll
-            for (int jj = 0; jj < kNb; ++jj) z[b] = csub(z[b], cmul(sYb[(row + b) * kNb + jj], Sv[jj]));
-          }
-#pragma unroll
-          for (int b = 0; b < kB; ++b) Z[(int64_t)(row + b) * n + tid] = z[b];
-        }
-        for (; row < n; ++row) {
-          cf z = Z[(int64_t)row * n + tid];
-#pragma unroll
-          for (int jj = 0; jj < kNb; ++jj) z = csub(z, cmul(sYb[row * kNb + jj], Sv[jj]));
-          Z[(int64_t)row * n + tid] = z;
-        }
-      }
+      if (tid < r) bt_vector(Z, n, tid, k0, sYb, sT);
       __syncthreads();
       continue;
     }
