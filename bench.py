@@ -37,7 +37,7 @@ WORKLOAD = "metric"
 # capture recorded in profiles/sense_four_pass_kernels_90x90x60.md; ncu
 # flushes L2 before each launch, so these are cold-cache upper bounds (the
 # timed loop finds most of the chunk's k-space in L2).
-TRAFFIC_PER_LAUNCH = {"pfwd": 80469248, "zmask": 142843648, "padj": 164751616, "csum": 114883072}
+TRAFFIC_PER_LAUNCH = {"pfwd": 80505600, "zmask": 140111872, "padj": 162665984, "csum": 113441024}
 
 
 def describe(pb) -> str:
