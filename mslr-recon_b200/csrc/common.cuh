@@ -63,6 +63,7 @@ struct ScaleGeom {
   // covering patch indices along d are [lo, hi] (inclusive); -1 if none
   int* d_cover;     // device: per dim, 2*N[d] ints
   int nsplit_tuned = 0;   // split-K count of the Gram chosen by the autotuner (0: heuristic)
+  int eig_big = 0;        // eigen stage in the 1024-thread CTA variant (autotuner; n > 384 always is)
   std::vector<int> h_starts;
 };
 

@@ -989,7 +989,9 @@ int eig_launch_group(const std::vector<const EigSegment*>& segs, const double* t
     total += e.np;
     nmax = std::max(nmax, e.n);
   }
-  const int threads = nmax <= kSmallT ? kSmallT : kT;
+  bool big = nmax > kSmallT;
+  for (const EigSegment* e : segs) big = big || e->big;
+  const int threads = big ? kT : kSmallT;
   a.rz = stage_cols(nmax, threads);
   const size_t sm = smem_bytes(nmax, threads, a.rz);
   if (threads == kSmallT)
@@ -1011,7 +1013,7 @@ int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int th
   if (nseg < 1 || nseg > kMaxSeg) return fail(MSLR_ERR_UNSUPPORTED, "too many scales in one launch");
   std::vector<const EigSegment*> small, big, all;
   for (int s = 0; s < nseg; ++s) {
-    (segs[s].n <= kSmallT ? small : big).push_back(&segs[s]);
+    (segs[s].n <= kSmallT && !segs[s].big ? small : big).push_back(&segs[s]);
     all.push_back(&segs[s]);
   }
   if (thr_per_patch || small.empty() || big.empty()) return eig_launch_group(all, thr, thr_per_patch, st);
@@ -1021,7 +1023,7 @@ int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int th
 }
 
 int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, const double* thr,
-                int thr_per_patch, double lam, cudaStream_t st) {
+                int thr_per_patch, double lam, cudaStream_t st, int big) {
   EigSegment s;
   s.n = n;
   s.np = np;
@@ -1030,6 +1032,7 @@ int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, cons
   s.aux = reinterpret_cast<double*>(aux);
   s.rank = rank;
   s.lam = lam;
+  s.big = big;
   s.nuc = nullptr;
   return eig_launch_multi(1, &s, thr, thr_per_patch, st);
 }

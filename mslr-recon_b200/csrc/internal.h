@@ -97,6 +97,7 @@ struct Ctx {
   bool spec_four = true;
   int spec_pfwd_ctas = 0, spec_zmask_ctas = 0, spec_padj_ctas = 0;
   bool spec_zmask1 = false;   // z-mask kernel variant with one CTA per SM
+  int spec_zmask_ctas_v[2] = {0, 0};   // resident CTAs of the two z-mask variants (two / one per SM)
   // chunks of the four-pass form alternate between two streams ("lanes",
   // each with its own k-space buffer) when spec_lanes == 2 (the default;
   // MSLR_SENSE_LANES=1 keeps one), so one chunk's kernels overlap the other's
@@ -223,6 +224,7 @@ struct EigSegment {
   double* aux;   // np × n × n scratch
   int* rank;     // np
   double lam;
+  int big = 0;             // 1: the 1024-thread CTA variant even when n <= 384
   double* nuc = nullptr;   // when set: per-patch Σ √λ above the threshold only (no vectors, no W)
   double* lam_out = nullptr;   // when set: every eigenpair — V (row-major, G = V Λ Vᴴ) in zv
                                // and the eigenvalues (descending, np × n) here; threshold unused
@@ -231,7 +233,7 @@ int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int th
                      cudaStream_t st);
 int eig2_prepare(int nmax);
 int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, const double* thr,
-                int thr_per_patch, double lam, cudaStream_t st);
+                int thr_per_patch, double lam, cudaStream_t st, int big = 0);
 
 // ---- cost evaluation (svst.cu, cost.cu) ------------------------------------------
 int patch_nucnorm_all(Ctx* c, const cf* X, double* reg_out, cudaStream_t st);
@@ -259,6 +261,8 @@ int set_scalar(double* dst, double v, cudaStream_t st);
 // ---- autotuner (api.cu; sense_spec.cu, svst.cu) ---------------------------------
 int tune_sense_chunks(Ctx* c, cudaStream_t st);
 int tune_svst_splits(Ctx* c, cudaStream_t st);
+int tune_sense_variants(Ctx* c, cudaStream_t st);
+int tune_eig_variants(Ctx* c, cudaStream_t st);
 int autotune(Ctx* c, cudaStream_t st);
 // milliseconds per call of fn(), timed with events on st after one warm-up call
 template <class Fn>

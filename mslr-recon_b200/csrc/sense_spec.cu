@@ -1169,21 +1169,24 @@ bool sense_spec_setup(Ctx* c) {
   if (c->spec_four) {
     const char* zc = std::getenv("MSLR_ZMASK_CTAS");
     c->spec_zmask1 = zc && std::string(zc) == "1";
-    const void* zk = c->spec_zmask1 ? o->zmask1 : o->zmask;
-    int a = 0, b = 0, d = 0;
+    int a = 0, b = 0, b1 = 0, d = 0;
     if (cudaFuncSetAttribute(o->pfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_pfwd) ||
-        cudaFuncSetAttribute(zk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zmask) ||
+        cudaFuncSetAttribute(o->zmask, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zmask) ||
+        cudaFuncSetAttribute(o->zmask1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zmask) ||
         cudaFuncSetAttribute(o->padj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_padj) ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, o->pfwd, o->xy_threads, o->smem_pfwd) ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, zk, o->zadj_threads, o->smem_zmask) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, o->zmask, o->zadj_threads, o->smem_zmask) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, o->zmask1, o->zadj_threads, o->smem_zmask) ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, o->padj, o->xy_threads, o->smem_padj) ||
-        a < 1 || b < 1 || d < 1 ||
+        a < 1 || b < 1 || b1 < 1 || d < 1 ||
         dalloc(c, (void**)&c->d_xsum, (size_t)c->Nt * c->nvox * sizeof(cf))) {
       cudaGetLastError();
       c->spec_four = false;
     } else {
       c->spec_pfwd_ctas = a * c->nsm;
-      c->spec_zmask_ctas = b * c->nsm;
+      c->spec_zmask_ctas_v[0] = b * c->nsm;
+      c->spec_zmask_ctas_v[1] = b1 * c->nsm;
+      c->spec_zmask_ctas = c->spec_zmask_ctas_v[c->spec_zmask1 ? 1 : 0];
       c->spec_padj_ctas = d * c->nsm;
       // two lanes by default (measured 8.65 → 7.77 ms for a 40-frame operator
       // at 90×90×60 × 18 coils); MSLR_SENSE_LANES=1 keeps one
@@ -1426,9 +1429,41 @@ int tune_sense_chunks(Ctx* c, cudaStream_t st) {
   return MSLR_OK;
 }
 
+// Autotuner, four-pass form: one or two lanes (streams) for the chunks, and
+// the z-mask kernel with two CTAs per SM (64 registers) or one (more
+// registers, fewer slabs in flight), timed on the chosen chunk shape.
+int tune_sense_variants(Ctx* c, cudaStream_t st) {
+  if (!c->spec || !c->spec_four || c->xy_tc) return MSLR_OK;
+  const int64_t E = (int64_t)c->Nt * c->nvox;
+  const int max_lanes = c->sn_stream ? 2 : 1;
+  float best = 1e30f;
+  int bl = c->spec_lanes, bz = c->spec_zmask1 ? 1 : 0;
+  for (int lanes = 1; lanes <= max_lanes; ++lanes) {
+    for (int z1 = 0; z1 <= 1; ++z1) {
+      c->spec_lanes = lanes;
+      c->spec_zmask1 = z1 == 1;
+      c->spec_zmask_ctas = c->spec_zmask_ctas_v[z1];
+      float ms = 0.f;
+      int rc = time_ms(st, 2, &ms, [&] { return normal_op_spec(c, c->d_ahy, 1, E, c->d_G, false, st); });
+      if (rc) return rc;
+      if (ms < best) {
+        best = ms;
+        bl = lanes;
+        bz = z1;
+      }
+    }
+  }
+  c->spec_lanes = bl;
+  c->spec_zmask1 = bz == 1;
+  c->spec_zmask_ctas = c->spec_zmask_ctas_v[bz];
+  return MSLR_OK;
+}
+
 int autotune(Ctx* c, cudaStream_t st) {
   int rc = tune_sense_chunks(c, st);
+  if (!rc) rc = tune_sense_variants(c, st);
   if (!rc) rc = tune_svst_splits(c, st);
+  if (!rc) rc = tune_eig_variants(c, st);
   if (c->gexec) {   // the captured iteration holds the old launch shapes
     cudaGraphExecDestroy(c->gexec);
     c->gexec = nullptr;

@@ -363,12 +363,12 @@ int svst_form_w(const WorkPtrs& w, int n, int64_t np, int tc, const DevWait& dw,
 // Gram → eig → W → (rebuild into out or pbuf) for all patches described by m.
 int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, int nsplit,
               const double* thr, int thr_per_patch, double lam, cf* out, int direct, int tc,
-              const DevWait& dw, cudaStream_t st, uint64_t* launches) {
+              const DevWait& dw, cudaStream_t st, uint64_t* launches, int eig_big = 0) {
   int rc = svst_gram(in, m, np, w, nsplit, tc, dw, st, launches);
   if (rc) return rc;
   if (launches) *launches += 1;
   rc = eig2_launch(m.n, np, w.gram, reinterpret_cast<cf*>(w.zv), reinterpret_cast<float*>(w.aux),
-                   w.rank, thr, thr_per_patch, lam, st);
+                   w.rank, thr, thr_per_patch, lam, st, eig_big);
   if (rc) return rc;
   if ((rc = svst_form_w(w, m.n, np, tc, dw, st, launches))) return rc;
   return svst_rebuild(in, m, np, w, out, direct, tc, dw, st, launches);
@@ -537,14 +537,14 @@ int patch_svst(Ctx* c, int s, const double* thr_dev, double lam, const cf* img_i
     cf* dst = img_out;
     if (img_in == img_out) dst = c->d_img_tmp;   // Gram/rebuild read the input throughout
     if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, thr_per_patch, lam, dst, 1, tc, ctx_wait(c), st,
-                        &c->launches)))
+                        &c->launches, g.eig_big)))
       return rc;
     if (dst != img_out)
       MSLR_CUDA_TRY(cudaMemcpyAsync(img_out, dst, (size_t)c->Nt * c->nvox * sizeof(cf),
                                     cudaMemcpyDeviceToDevice, st));
   } else {
     if ((rc = svst_core(img_in, m, g.Np, w, nsplit, thr_dev, thr_per_patch, lam, c->d_pbuf, 0, tc,
-                        ctx_wait(c), st, &c->launches)))
+                        ctx_wait(c), st, &c->launches, g.eig_big)))
       return rc;
     k_recombine<<<1184, 256, 0, st>>>(c->d_pbuf, m, g.d_cover, img_out);
     MSLR_CUDA_TRY(cudaGetLastError());
@@ -726,11 +726,12 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     segs[k].aux = ws[k].aux;
     segs[k].rank = ws[k].rank;
     segs[k].lam = c->lambdas[k];
+    segs[k].big = g.eig_big;
   }
   if ((rc = eig_launch_multi(c->Ns, segs.data(), thr_dev, 0, st))) return rc;
   {
     bool small = false, big = false;   // one eigen launch per CTA variant present
-    for (const auto& sg : segs) (sg.n <= 384 ? small : big) = true;
+    for (const auto& sg : segs) (sg.n <= 384 && !sg.big ? small : big) = true;
     c->launches += (small && big) ? 2 : 1;
   }
   for (int k = 0; k < c->Ns; ++k)
@@ -1069,6 +1070,39 @@ int tune_svst_splits(Ctx* c, cudaStream_t st) {
       if (ns == 1) break;
     }
     g.nsplit_tuned = bs;
+  }
+  return MSLR_OK;
+}
+
+// Eigen-stage CTA variant of each scale whose Gram side allows both (n <= 384):
+// 384 threads, two patches per SM, or 1024 threads, one per SM — timed on the
+// scale's patch SVST of A'y at the threshold 1/Ns · λ_k (a first POGM
+// iteration's ζ·λ_k with σ1 = 1), into the POGM z buffer (scratch until the
+// first step).
+int tune_eig_variants(Ctx* c, cudaStream_t st) {
+  double* thr = c->d_thr + 3;
+  if (int rc = set_scalar(thr, 1.0 / (double)c->Ns, st)) return rc;
+  for (size_t k = 0; k < c->scales.size(); ++k) {
+    ScaleGeom& g = c->scales[k];
+    if (g.n > 384) {
+      g.eig_big = 0;
+      continue;
+    }
+    float best = 1e30f;
+    int bb = 0;
+    for (int big = 0; big <= 1; ++big) {
+      g.eig_big = big;
+      float ms = 0.f;
+      int rc = time_ms(st, 2, &ms, [&] {
+        return patch_svst(c, (int)k, thr, c->lambdas[k], c->d_ahy, c->d_Z, st, 0);
+      });
+      if (rc) return rc;
+      if (ms < best) {
+        best = ms;
+        bb = big;
+      }
+    }
+    g.eig_big = bb;
   }
   return MSLR_OK;
 }

@@ -439,8 +439,9 @@ def test_mixed_gram_sides_per_iteration(torch, M):
 
 
 def test_autotune_keeps_parity(torch, M, small_problem):
-    """The autotuner's choices (SENSE chunk shape, Gram split counts) are valid
-    and the tuned iteration still matches the FP64 oracle."""
+    """The autotuner's choices (SENSE chunk shape, lanes and z-mask variant,
+    Gram split counts, eigen CTA variants) are valid and the tuned iteration
+    still matches the FP64 oracle."""
     pb = small_problem
     Nt, Nc, K = pb["y"].shape
     niter = 6
@@ -454,6 +455,9 @@ def test_autotune_keeps_parity(torch, M, small_problem):
         t = ctx.autotune()
         assert t["coils_per_group"] in (2, 3, 4, 6, 8) and 1 <= t["frames_per_chunk"] <= 4
         assert len(t["gram_splits"]) == len(pb["patch_sizes"])
+        assert t["lanes"] in (1, 2) and t["zmask_ctas_per_sm"] in (1, 2)
+        assert len(t["eig_threads"]) == len(pb["patch_sizes"])
+        assert all(v in (384, 1024) for v in t["eig_threads"])
         X = ctx.init_x0()
         ctx.pogm_begin(X, niter, L=1.0)
         errs = []
