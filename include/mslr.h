@@ -371,7 +371,8 @@ int mslr_pogm_grad(mslr_ctx* ctx, const void* X_true, int32_t niter, double L, d
 /* Autotuner (tuned and TF32 forms; no counterpart in the reference).  Times,
  * on the bound context, the launch shapes the library can choose freely —
  * coils per group × frames per chunk of the SENSE normal operator, its lanes
- * (one or two streams) and z-mask CTA variant (two or one per SM), the
+ * (one or two streams) and z-mask CTA variant (two per SM, one per SM, or
+ * two per SM of fewer warps), the
  * split-K count of each single-patch scale's Gram, and the eigen stage's CTA
  * variant of each scale with Gram side <= 384 (384 threads, two per SM, or
  * 1024 threads) — and keeps the fastest.  Runs at the end of mslr_bind when
@@ -380,7 +381,8 @@ int mslr_pogm_grad(mslr_ctx* ctx, const void* X_true, int32_t niter, double L, d
  * before the first POGM step (it uses the POGM buffers as scratch), or the
  * captured iteration is captured again.  mslr_get_tuning writes {coils per
  * group, frames per chunk, split count of scale 0 .. Ns−1 (0: heuristic),
- * lanes, z-mask CTAs per SM, eigen CTA threads of scale 0 .. Ns−1}. */
+ * lanes, z-mask CTAs per SM, z-mask warps per CTA, eigen CTA threads of
+ * scale 0 .. Ns−1}. */
 int mslr_autotune(mslr_ctx* ctx, void* stream);
 int mslr_get_tuning(const mslr_ctx* ctx, int32_t* values, int32_t cap, int32_t* count);
 

@@ -339,14 +339,15 @@ class MSLRContext:
 
     def tuning(self):
         """{'coils_per_group', 'frames_per_chunk', 'gram_splits': [per scale, 0 = heuristic],
-        'lanes', 'zmask_ctas_per_sm', 'eig_threads': [per scale]}"""
+        'lanes', 'zmask_ctas_per_sm', 'zmask_warps', 'eig_threads': [per scale]}"""
         n = C.c_int32()
         vals = (C.c_int32 * 64)()
         self._chk(lib.mslr_get_tuning(self._h, vals, 64, C.byref(n)))
         v = list(vals[:n.value])
         ns = self.Ns
         return {"coils_per_group": v[0], "frames_per_chunk": v[1], "gram_splits": v[2:2 + ns],
-                "lanes": v[2 + ns], "zmask_ctas_per_sm": v[3 + ns], "eig_threads": v[4 + ns:4 + 2 * ns]}
+                "lanes": v[2 + ns], "zmask_ctas_per_sm": v[3 + ns], "zmask_warps": v[4 + ns],
+                "eig_threads": v[5 + ns:5 + 2 * ns]}
 
     def set_lambdas(self, lambdas):
         """Per-scale weights λ_k of g_prox (scripts/reconstruct.jl:164-169, 196-202)."""

@@ -599,7 +599,8 @@ int mslr_get_tuning(const mslr_ctx* ctx, int32_t* values, int32_t cap, int32_t* 
   std::vector<int32_t> v = {ctx->spec_ch, ctx->spec_fr};
   for (const auto& g : ctx->scales) v.push_back(g.nsplit_tuned > 0 ? g.nsplit_tuned : 0);
   v.push_back(ctx->spec_lanes);
-  v.push_back(ctx->spec_zmask1 ? 1 : 2);
+  v.push_back(ctx->spec_zmask_var == 1 ? 1 : 2);
+  v.push_back(ctx->spec_zmask_warps[ctx->spec_zmask_var]);
   for (const auto& g : ctx->scales) v.push_back(g.n > 384 || g.eig_big ? 1024 : 384);
   *count = (int32_t)v.size();
   for (int32_t i = 0; i < cap && i < (int32_t)v.size(); ++i) values[i] = v[i];

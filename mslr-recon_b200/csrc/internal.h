@@ -96,8 +96,11 @@ struct Ctx {
   // summed image Σ_k X_k of all frames that its forward plane pass reads
   bool spec_four = true;
   int spec_pfwd_ctas = 0, spec_zmask_ctas = 0, spec_padj_ctas = 0;
-  bool spec_zmask1 = false;   // z-mask kernel variant with one CTA per SM
-  int spec_zmask_ctas_v[2] = {0, 0};   // resident CTAs of the two z-mask variants (two / one per SM)
+  // z-mask kernel variant: 0 two CTAs per SM (64 registers), 1 one CTA per SM
+  // (MSLR_ZMASK_CTAS=1), 2 two CTAs per SM with fewer warps (more registers)
+  int spec_zmask_var = 0;
+  int spec_zmask_ctas_v[3] = {0, 0, 0};   // resident CTAs of each variant
+  int spec_zmask_warps[3] = {0, 0, 0};    // warps per CTA of each variant
   // chunks of the four-pass form alternate between two streams ("lanes",
   // each with its own k-space buffer) when spec_lanes == 2 (the default;
   // MSLR_SENSE_LANES=1 keeps one), so one chunk's kernels overlap the other's

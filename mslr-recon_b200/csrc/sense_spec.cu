@@ -76,6 +76,15 @@ struct Shape {
   static constexpr int ev(int n) { return (n + 1) & ~1; }
   // warps of the adjoint z kernel (two CTAs per SM): at most 16
   static constexpr int ZW2 = mn(16, cdiv(NX, AZ::LPW));
+  // fewer warps for the z-mask kernel's third variant (more registers per
+  // thread at two CTAs per SM): the most, at most 12, whose compute warps
+  // divide the slab's line groups evenly (warp 0 then only moves slabs)
+  static constexpr int zwm(int g) {
+    int w = 12;
+    while (w > 2 && g % (w - 1) != 0) --w;
+    return (w > 2) ? w : mn(12, g);
+  }
+  static constexpr int ZWm = mn(ZW2, zwm(cdiv(NX, AZ::LPW)));
   static constexpr size_t smem_zfwd = sizeof(cf) * (4 * (size_t)S + ev(NZ)) + 3 * sizeof(uint64_t);
   static constexpr size_t smem_zadj = sizeof(cf) * (2 * (size_t)S + ev(NZ)) + sizeof(uint64_t);
   static constexpr size_t smem_xy =
@@ -584,15 +593,15 @@ __global__ void __launch_bounds__(Sh::XYW * 32, 1)
 // words of the next slab are staged (double-buffered) while the current one
 // finishes, so a unit needs one block barrier.  MINB: CTAs per SM the
 // register budget is set for.
-template <class Sh, int MINB>
-__global__ void __launch_bounds__(Sh::ZW2 * 32, MINB)
+template <class Sh, int MINB, int NW = Sh::ZW2>
+__global__ void __launch_bounds__(NW * 32, MINB)
     k_zmask(cf* __restrict__ T, const uint32_t* __restrict__ mask, int nwords, int t0, int nf, int ch,
             const cf* __restrict__ twz_g, int* __restrict__ err) {
   using AZ = typename Sh::AZ;
   constexpr int NX = Sh::NX, NY = Sh::NY, NZ = Sh::NZ, S = Sh::S, PL = Sh::PL;
   constexpr int64_t NVOX = Sh::NVOX;
   constexpr int kGroups = Sh::cdiv(NX, AZ::LPW);   // line groups of a slab
-  constexpr bool kCopyWarp = Sh::ZW2 > 1 && kGroups % (Sh::ZW2 - 1) == 0;
+  constexpr bool kCopyWarp = NW > 1 && kGroups % (NW - 1) == 0;
   extern __shared__ __align__(128) unsigned char smraw[];
   cf* SL = reinterpret_cast<cf*>(smraw);          // two slab buffers
   cf* tf = SL + 2 * S;                            // twiddle tables: forward (the fused pass)
@@ -1072,6 +1081,8 @@ struct SpecOps {
   const void* pfwd;
   const void* zmask;     // two CTAs per SM (64 registers)
   const void* zmask1;    // one CTA per SM (more registers, MSLR_ZMASK_CTAS=1)
+  const void* zmaskm;    // two CTAs per SM with Sh::ZWm warps (more registers per thread)
+  int zmaskm_threads;
   const void* padj;
   size_t smem_pfwd, smem_zmask, smem_padj;
   const void* xy_tc;                       // tensor-core plane pass (square planes), or null
@@ -1096,6 +1107,8 @@ SpecOps ops_of() {
             reinterpret_cast<const void*>(&k_pfwd<Sh>),
             reinterpret_cast<const void*>(&k_zmask<Sh, 2>),
             reinterpret_cast<const void*>(&k_zmask<Sh, 1>),
+            reinterpret_cast<const void*>(&k_zmask<Sh, 2, Sh::ZWm>),
+            Sh::ZWm * 32,
             reinterpret_cast<const void*>(&k_padj<Sh>),
             Sh::smem_pfwd,
             Sh::smem_zmask,
@@ -1168,17 +1181,19 @@ bool sense_spec_setup(Ctx* c) {
   }
   if (c->spec_four) {
     const char* zc = std::getenv("MSLR_ZMASK_CTAS");
-    c->spec_zmask1 = zc && std::string(zc) == "1";
-    int a = 0, b = 0, b1 = 0, d = 0;
+    c->spec_zmask_var = (zc && std::string(zc) == "1") ? 1 : 0;
+    int a = 0, b = 0, b1 = 0, bm = 0, d = 0;
     if (cudaFuncSetAttribute(o->pfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_pfwd) ||
         cudaFuncSetAttribute(o->zmask, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zmask) ||
         cudaFuncSetAttribute(o->zmask1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zmask) ||
+        cudaFuncSetAttribute(o->zmaskm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_zmask) ||
         cudaFuncSetAttribute(o->padj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)o->smem_padj) ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, o->pfwd, o->xy_threads, o->smem_pfwd) ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, o->zmask, o->zadj_threads, o->smem_zmask) ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, o->zmask1, o->zadj_threads, o->smem_zmask) ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bm, o->zmaskm, o->zmaskm_threads, o->smem_zmask) ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d, o->padj, o->xy_threads, o->smem_padj) ||
-        a < 1 || b < 1 || b1 < 1 || d < 1 ||
+        a < 1 || b < 1 || b1 < 1 || bm < 1 || d < 1 ||
         dalloc(c, (void**)&c->d_xsum, (size_t)c->Nt * c->nvox * sizeof(cf))) {
       cudaGetLastError();
       c->spec_four = false;
@@ -1186,7 +1201,10 @@ bool sense_spec_setup(Ctx* c) {
       c->spec_pfwd_ctas = a * c->nsm;
       c->spec_zmask_ctas_v[0] = b * c->nsm;
       c->spec_zmask_ctas_v[1] = b1 * c->nsm;
-      c->spec_zmask_ctas = c->spec_zmask_ctas_v[c->spec_zmask1 ? 1 : 0];
+      c->spec_zmask_ctas_v[2] = bm * c->nsm;
+      c->spec_zmask_warps[0] = c->spec_zmask_warps[1] = o->zadj_threads / 32;
+      c->spec_zmask_warps[2] = o->zmaskm_threads / 32;
+      c->spec_zmask_ctas = c->spec_zmask_ctas_v[c->spec_zmask_var];
       c->spec_padj_ctas = d * c->nsm;
       // two lanes by default (measured 8.65 → 7.77 ms for a 40-frame operator
       // at 90×90×60 × 18 coils); MSLR_SENSE_LANES=1 keeps one
@@ -1257,7 +1275,9 @@ static int normal_op_four(Ctx* c, const SpecOps* o, const cf* X, int ns, int64_t
   cf* T = c->d_T;
   int* err = c->d_err;
   const int sub = subtract ? 1 : 0;
-  const void* zk = c->spec_zmask1 ? o->zmask1 : o->zmask;
+  const int zv = c->spec_zmask_var;
+  const void* zk = zv == 1 ? o->zmask1 : zv == 2 ? o->zmaskm : o->zmask;
+  const int zthreads = zv == 2 ? o->zmaskm_threads : o->zadj_threads;
   c->prof_kernels = 4;
   // two lanes: chunk j of every group on lane j % 2 (so the += of later
   // groups stays ordered after the first group's chunk of the same frames),
@@ -1293,7 +1313,7 @@ static int normal_op_four(Ctx* c, const SpecOps* o, const cf* X, int ns, int64_t
         const int grid = std::max(1, std::min(slabs, c->spec_zmask_ctas));
         void* args[] = {(void*)&T, (void*)&mask, (void*)&nwords, (void*)&t0, (void*)&f, (void*)&ch,
                         (void*)&c->d_tw[2], (void*)&err};
-        MSLR_CUDA_TRY(cudaLaunchKernel(zk, dim3(grid), dim3(o->zadj_threads), args, o->smem_zmask, st));
+        MSLR_CUDA_TRY(cudaLaunchKernel(zk, dim3(grid), dim3(zthreads), args, o->smem_zmask, st));
       }
       if (int rc = prof_mark(c, st)) return rc;
       {
@@ -1430,18 +1450,19 @@ int tune_sense_chunks(Ctx* c, cudaStream_t st) {
 }
 
 // Autotuner, four-pass form: one or two lanes (streams) for the chunks, and
-// the z-mask kernel with two CTAs per SM (64 registers) or one (more
-// registers, fewer slabs in flight), timed on the chosen chunk shape.
+// the z-mask kernel variant — two CTAs per SM (64 registers), one CTA per SM
+// (more registers, fewer slabs in flight), or two CTAs per SM of fewer warps
+// (more registers per thread) — timed on the chosen chunk shape.
 int tune_sense_variants(Ctx* c, cudaStream_t st) {
   if (!c->spec || !c->spec_four || c->xy_tc) return MSLR_OK;
   const int64_t E = (int64_t)c->Nt * c->nvox;
   const int max_lanes = c->sn_stream ? 2 : 1;
   float best = 1e30f;
-  int bl = c->spec_lanes, bz = c->spec_zmask1 ? 1 : 0;
+  int bl = c->spec_lanes, bz = c->spec_zmask_var;
   for (int lanes = 1; lanes <= max_lanes; ++lanes) {
-    for (int z1 = 0; z1 <= 1; ++z1) {
+    for (int z1 = 0; z1 <= 2; ++z1) {
       c->spec_lanes = lanes;
-      c->spec_zmask1 = z1 == 1;
+      c->spec_zmask_var = z1;
       c->spec_zmask_ctas = c->spec_zmask_ctas_v[z1];
       float ms = 0.f;
       int rc = time_ms(st, 2, &ms, [&] { return normal_op_spec(c, c->d_ahy, 1, E, c->d_G, false, st); });
@@ -1454,7 +1475,7 @@ int tune_sense_variants(Ctx* c, cudaStream_t st) {
     }
   }
   c->spec_lanes = bl;
-  c->spec_zmask1 = bz == 1;
+  c->spec_zmask_var = bz;
   c->spec_zmask_ctas = c->spec_zmask_ctas_v[bz];
   return MSLR_OK;
 }
