@@ -18,7 +18,9 @@
 //      shuffle transpose-reduction, both stored per tile and summed per row
 //      in a fixed order, so results are bit-reproducible), streaming the
 //      trailing triangle once per step; the working set of ~300 resident
-//      patches stays in L2.
+//      patches stays in L2.  The pass also leaves the next column in shared
+//      memory, and every thread computes the reflector scalars and the next
+//      pivot row's (v, w) itself, so a step has four block barriers.
 //   2. Eigenvalues of T above β² by bisection on FP64 Sturm counts, one
 //      thread per eigenvalue.
 //   3. Eigenvectors of T by FP64 twisted factorisation, one thread per
@@ -31,8 +33,15 @@
 //      columns beyond the rank set to zero.
 // Zero patches give no eigenvalue above β² and Ṽ = 0, hence W = 0 (the
 // reference's zero-norm skip, src/recon.jl:185).
+//
+// Split stage (thresholded SVSTs with 64 <= n <= 384): three launches instead
+// of one, so that each phase runs at the occupancy it needs — phase 1 and the
+// WY blocks' T factors (two CTAs per SM), phases 2–3 (four CTAs per SM, all
+// patches resident at once), and phases 4–5 as k_wy_apply: 32 eigenvectors
+// of one patch per CTA, held in registers through every block update.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "internal.h"
@@ -45,6 +54,7 @@ constexpr int kT = 1024;   // most threads per CTA (one row / eigenvalue per thr
 constexpr int kSmallT = 384;   // CTA size for n <= 384: two patches share an SM
 constexpr int kNb = 16;    // reflectors per WY block
 constexpr int kCW = 16;    // eigenvectors per back-transform pass
+constexpr int kPairsMinB = 4;   // CTAs per SM of the split stage's eigenpair launch
 
 __device__ __forceinline__ float warp_sum(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -120,6 +130,7 @@ struct Seg {
   double lam;      // threshold multiplier of the segment (λ_k)
   double* nuc;     // values-only mode when set: np sums Σ √λ_i over λ_i above β², no vectors
   double* lam_out; // full mode when set: all n eigenpairs, V unscaled in zv, λ (descending) here
+  double* side;    // split stage: np × 6n — d, e (FP64), λ, h of the tridiagonal (k_eig modes 1, 2)
 };
 
 constexpr int kMaxSeg = 8;
@@ -142,7 +153,7 @@ size_t part_bytes(int n) {
 
 size_t vec_bytes(int n) {
   const size_t np = (size_t)n + 32;
-  return np * sizeof(float4) + 4 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
+  return np * sizeof(float4) + 5 * np * sizeof(cf) + 4 * (size_t)n * sizeof(double) +
          3 * (size_t)n * sizeof(float) + 64 * sizeof(float) + 64 * sizeof(double);
 }
 
@@ -235,7 +246,8 @@ __device__ __forceinline__ void col_sums(float* cr, float* ci, int lane) {
 // the second group).
 template <bool PIPE>
 __device__ __noinline__ void full_tile(cf* A, int n, int o, int I, int J, int t, int lane, const float4* spw,
-                                       const cf* svr, const cf* svp, const cf* swp, const cf* sv, cf* part) {
+                                       const cf* svr, const cf* svp, const cf* swp, const cf* sv, cf* part,
+                                       cf* scol) {
   const int row = o + I * 32 + lane;
   const cf vpr = svp[row], wpr = swp[row], vr = sv[row];
   float yr = 0.f, yim = 0.f;
@@ -262,6 +274,7 @@ __device__ __noinline__ void full_tile(cf* A, int n, int o, int I, int J, int t,
     }
     float cr[8], ci[8];
     tile_group(a, pw + g8 * 8, vv + g8 * 4, vpr, wpr, vr, yr, yim, cr, ci);
+    if (scol && g8 == 0) scol[row] = a[0];   // column o, the next step's
 #pragma unroll
     for (int b = 0; b < 8; ++b) col0[(int64_t)(g8 * 8 + b) * n] = a[b];
     col_sums(cr, ci, lane);
@@ -336,7 +349,80 @@ __device__ __noinline__ void bt_vector(cf* Z, int n, int col, int k0, const cf* 
   for (; row < n; ++row) Z[(int64_t)row * n + col] = upd(row, Z[(int64_t)row * n + col]);
 }
 
-template <int MAXT, int MINB>
+// Upper-triangle slot q (column by column, column c holding rows 0..c−1) of a
+// column-major n × n matrix: the split stage keeps the WY blocks' T factors in
+// the strictly upper triangle of the patch's Gram buffer, which nothing reads
+// between the tridiagonalisation and the back-transform (the W Gram rewrites
+// the whole buffer afterwards).
+__device__ __forceinline__ int64_t upper_slot(int n, int q) {
+  int c = (int)((1.f + sqrtf(1.f + 8.f * (float)q)) * 0.5f);
+  while (c > 1 && c * (c - 1) / 2 > q) --c;
+  while ((c + 1) * c / 2 <= q) ++c;
+  return (int64_t)c * n + (q - c * (c - 1) / 2);
+}
+
+// T factors (zlarft, forward columnwise) of the WY blocks of kNb reflectors,
+// taken from the last reflector down as the back-transform applies them;
+// block blk = (n − 1 − kend) / kNb goes to upper slots [256·blk, 256·blk + 256).
+// sYb: n × kNb complex scratch followed by two kNb × kNb blocks.
+__device__ void wy_factors(cf* A, int n, const float* taur, const float* taui, cf* sYb, int tid, int kT) {
+  cf* sT = sYb + (int64_t)n * kNb;
+  cf* sYY = sT + kNb * kNb;
+  const int nref = n - 1;
+  for (int kend = nref; kend > 0; kend -= kNb) {
+    const int k0 = max(0, kend - kNb);
+    const int nb = kend - k0;
+    const int blk = (nref - kend) / kNb;
+    const int m = n - k0 - 1;
+    for (int q = tid; q < m * kNb; q += kT) {   // rows k0+1 .. n−1 of reflectors k0 .. k0+nb−1
+      const int jj = q / m, row = k0 + 1 + (q - jj * m);
+      const int k = k0 + jj;
+      cf y = make_float2(0.f, 0.f);
+      if (jj < nb) {
+        if (row == k + 1) y = make_float2(1.f, 0.f);
+        else if (row > k + 1) y = __ldcg(A + (int64_t)k * n + row);
+      }
+      sYb[row * kNb + jj] = y;
+    }
+    __syncthreads();
+    if (tid < kNb * kNb) {   // Yᴴ Y
+      const int a = tid / kNb, b = tid - a * kNb;
+      float sr = 0.f, si = 0.f;
+      for (int row = k0 + 1; row < n; ++row) {
+        const cf ya = sYb[row * kNb + a], yb = sYb[row * kNb + b];
+        sr += ya.x * yb.x + ya.y * yb.y;
+        si += ya.x * yb.y - ya.y * yb.x;
+      }
+      sYY[tid] = make_float2(sr, si);
+    }
+    __syncthreads();
+    if (tid < 32) {   // lane a owns row a of T
+      const int a = tid;
+      for (int jj = 0; jj < kNb; ++jj) {
+        const cf tj = (jj < nb) ? make_float2(taur[k0 + jj], taui[k0 + jj]) : make_float2(0.f, 0.f);
+        if (a < jj) {
+          cf sacc = make_float2(0.f, 0.f);
+          for (int b = a; b < jj; ++b) sacc = cadd(sacc, cmul(sT[a * kNb + b], sYY[b * kNb + jj]));
+          const cf v = cmul(tj, sacc);
+          sT[a * kNb + jj] = make_float2(-v.x, -v.y);
+        } else if (a < kNb) {
+          sT[a * kNb + jj] = (a == jj) ? tj : make_float2(0.f, 0.f);
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    for (int t = tid; t < kNb * kNb; t += kT) A[upper_slot(n, blk * kNb * kNb + t)] = sT[t];
+    __syncthreads();
+  }
+}
+
+// MODE 0: the whole stage in one launch.  The split stage (three launches):
+// MODE 1 tridiagonalises and writes d, e to the side buffer and the WY
+// blocks' T factors to the Gram's upper triangle; MODE 2 computes the
+// eigenpairs of T from the side buffer (vectors into zv, FP32, [row][vector],
+// λ and h back to the side buffer); k_wy_apply then forms Ṽ.
+template <int MAXT, int MINB, int MODE>
 __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   extern __shared__ __align__(16) unsigned char smraw[];
   int s = 0;
@@ -365,13 +451,14 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   cf* sv = svr + npad;                              // v of this step  [npad]
   cf* svp = sv + npad;                              // previous v      [npad]
   cf* swp = svp + npad;                             // previous w      [npad]
-  float* hv = reinterpret_cast<float*>(swp + npad); // h               [n]
+  cf* scol = swp + npad;                            // next column     [npad]
+  float* hv = reinterpret_cast<float*>(scol + npad); // h              [n]
   float* taur = hv + n;                             // τ               [n]
   float* taui = taur + n;                           //                 [n]
   float* red0 = taui + n;                           // 2 × 32 floats
   float* red1 = red0 + 32;
   cf* sY = reinterpret_cast<cf*>((reinterpret_cast<uintptr_t>(red1 + 32) + 15) & ~(uintptr_t)15);
-  __shared__ float s_bc[4];
+  __shared__ cf s_x;
   __shared__ double s_bd[4];
   __shared__ int s_r;
 
@@ -380,6 +467,19 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   const float beta = (float)beta_d;
   (void)beta;
 
+  const int i = tid;   // row owned by this thread (n <= kT)
+  const int warp = tid >> 5, lane = tid & 31, nwarp = kT >> 5;
+  if constexpr (MODE == 2) {   // T from the side buffer (the same FP64 values phase 1 keeps)
+    const double* side = S.side + ip * 6 * (int64_t)n;
+    for (int q = tid; q < n; q += kT) {
+      dd[q] = side[q];
+      const double e = side[n + q];
+      ee[q] = e;
+      ee2[q] = e * e;
+    }
+    (void)nwarp;
+    __syncthreads();
+  } else {
   // ---- 1. tridiagonalisation with delayed rank-2 updates ---------------------
   for (int q = tid; q < npad; q += kT) {
     sv[q] = make_float2(0.f, 0.f);
@@ -389,31 +489,35 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     spw[q] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
-  const int i = tid;   // row owned by this thread (n <= kT)
-  const int warp = tid >> 5, lane = tid & 31, nwarp = kT >> 5;
   // per-tile row / column sums of the Hermitian matvec of a step: shared
   // memory (sharing the WY blocks' storage) for the 384-thread variant, the
   // patch's FP64 pivot scratch (idle until phase 3) for the large variant
   cf* part = (MAXT <= kSmallT) ? sY : reinterpret_cast<cf*>(AUX);
+  // (vp, wp) of the pivot row k, known to every thread: row k's entries of the
+  // previous step's v (1 when it reflected) and w (τ y_k − c), the latter from
+  // the row sums every thread adds up itself, so no barrier publishes them
+  cf vpk = make_float2(0.f, 0.f), wpk = make_float2(0.f, 0.f);
   for (int k = 0; k < n - 1; ++k) {
-    // current column k and diagonal k: stored − (vp wpᴴ + wp vpᴴ)
+    // current column k and diagonal k: stored − (vp wpᴴ + wp vpᴴ); after the
+    // first step the previous pass left the stored column in scol
     cf x = make_float2(0.f, 0.f);
     cf vpi = make_float2(0.f, 0.f), wpi = make_float2(0.f, 0.f);
     if (i < n) {
       vpi = svp[i];
       wpi = swp[i];
     }
-    const cf vpk = svp[k], wpk = swp[k];
     if (i >= k && i < n) {
-      x = __ldcg(A + (int64_t)k * n + i);
+      x = (k == 0) ? __ldcg(A + i) : scol[i];
       x = csub(x, cadd(cmul(vpi, cconj(wpk)), cmul(wpi, cconj(vpk))));
       if (i == k) dd[k] = (double)x.x;
     }
-    const float xn = block_sum((i >= k + 2 && i < n) ? cabs2(x) : 0.f, (k & 1) ? red1 : red0);
-    if (i == k + 1) {
-      // zlarfg: Hᴴ (α, x) = (β, 0), H = I − τ v vᴴ, β real
-      const float ar = x.x, ai = x.y;
-      float bt, tr, ti, sr, si;
+    if (i == k + 1) s_x = x;
+    const float xn = block_sum((i >= k + 2 && i < n) ? cabs2(x) : 0.f, red0);
+    // zlarfg, by every thread on the same values: Hᴴ (α, x) = (β, 0), H = I − τ v vᴴ, β real
+    float tr, ti, sr, si;
+    {
+      const float ar = s_x.x, ai = s_x.y;
+      float bt;
       if (xn == 0.f && ai == 0.f) {
         bt = ar;
         tr = ti = 0.f;
@@ -428,18 +532,15 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
         sr = zr / den;
         si = -zi / den;
       }
-      ee[k] = (double)bt;
-      ee2[k] = (double)bt * (double)bt;
-      taur[k] = tr;
-      taui[k] = ti;
-      s_bc[0] = tr;
-      s_bc[1] = ti;
-      s_bc[2] = sr;
-      s_bc[3] = si;
+      if (i == k + 1) {
+        ee[k] = (double)bt;
+        ee2[k] = (double)bt * (double)bt;
+        taur[k] = tr;
+        taui[k] = ti;
+      }
     }
-    __syncthreads();
-    const cf tau = make_float2(s_bc[0], s_bc[1]);
-    const cf scal = make_float2(s_bc[2], s_bc[3]);
+    const cf tau = make_float2(tr, ti);
+    const cf scal = make_float2(sr, si);
     const bool refl = (tau.x != 0.f || tau.y != 0.f);
     cf vi = make_float2(0.f, 0.f);
     if (i == k + 1) {
@@ -463,7 +564,8 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
         while (I * (I + 1) / 2 > t) --I;
         const int J = t - I * (I + 1) / 2;
         if (I != J && o + I * 32 + 32 <= n) {
-          full_tile<(MAXT <= kSmallT)>(A, n, o, I, J, t, lane, spw, svr, svp, swp, sv, part);
+          full_tile<(MAXT <= kSmallT)>(A, n, o, I, J, t, lane, spw, svr, svp, swp, sv, part,
+                                       J == 0 ? scol : nullptr);
           continue;
         }
         const bool diag = (I == J);
@@ -507,6 +609,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
             const int j = jb + b;
             if (rowok && j < n && (!diag || row >= j)) col0[(int64_t)(g8 * 8 + b) * n] = a[b];
           }
+          if (J == 0 && g8 == 0 && rowok) scol[row] = a[0];   // column o, the next step's
           // column sums over the 32 lanes: lane l ends with the sum of column l/4
           const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
 #pragma unroll
@@ -541,30 +644,52 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     }
     __syncthreads();
     // y_i in a fixed order: the row sums of tiles (I, 0..I), then the column
-    // sums of tiles (I..T-1, I) — the same bits on every run
-    float yr = 0.f, yi = 0.f;
-    if (i >= k + 1 && i < n) {
+    // sums of tiles (I..T-1, I) — the same bits on every run; every thread
+    // also adds up y of row k + 1 (the next pivot row) in the same order
+    float yr = 0.f, yi = 0.f, y1r = 0.f, y1i = 0.f;
+    {
       const int o = k + 1, T = (n - o + 31) >> 5;
-      const int I = (i - o) >> 5, l = (i - o) & 31;
-      const int t0 = I * (I + 1) / 2;
-      for (int J = 0; J <= I; ++J) {
-        const cf v = part[2 * (t0 + J) * 32 + l];
-        yr += v.x;
-        yi += v.y;
+      if (i >= k + 1 && i < n) {
+        const int I = (i - o) >> 5, l = (i - o) & 31;
+        const int t0 = I * (I + 1) / 2;
+        for (int J = 0; J <= I; ++J) {
+          const cf v = part[2 * (t0 + J) * 32 + l];
+          yr += v.x;
+          yi += v.y;
+        }
+        for (int I2 = I; I2 < T; ++I2) {
+          const cf v = part[(2 * (I2 * (I2 + 1) / 2 + I) + 1) * 32 + l];
+          yr += v.x;
+          yi += v.y;
+        }
       }
-      for (int I2 = I; I2 < T; ++I2) {
-        const cf v = part[(2 * (I2 * (I2 + 1) / 2 + I) + 1) * 32 + l];
-        yr += v.x;
-        yi += v.y;
+      {
+        const cf v = part[0];
+        y1r += v.x;
+        y1i += v.y;
+      }
+      for (int I2 = 0; I2 < T; ++I2) {
+        const cf v = part[(2 * (I2 * (I2 + 1) / 2)) * 32 + 32];
+        y1r += v.x;
+        y1i += v.y;
       }
     }
     // vᴴ y (real for Hermitian A)
-    const float vy = block_sum((i >= k + 1 && i < n) ? (vi.x * yr + vi.y * yi) : 0.f,
-                               (k & 1) ? red0 : red1);
+    const float vy = block_sum((i >= k + 1 && i < n) ? (vi.x * yr + vi.y * yi) : 0.f, red1);
     const float c = 0.5f * (tau.x * tau.x + tau.y * tau.y) * vy;
+    // the next pivot row's (vp, wp); thread k + 1 stores these same values
+    if (refl) {
+      const cf ty = cmul(tau, make_float2(y1r, y1i));
+      vpk = make_float2(1.f, 0.f);
+      wpk = make_float2(ty.x - c, ty.y);
+    } else {
+      vpk = wpk = make_float2(0.f, 0.f);
+    }
     if (i < n) {
       cf w = make_float2(0.f, 0.f);
-      if (i >= k + 1 && refl) {
+      if (i == k + 1) {
+        w = wpk;
+      } else if (i > k + 1 && refl) {
         const cf ty = cmul(tau, make_float2(yr, yi));
         w = make_float2(ty.x - c * vi.x, ty.y - c * vi.y);
       }
@@ -575,7 +700,9 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
         spw[i - k - 2] = make_float4(vq.x, vq.y, w.x, w.y);
       }
     }
-    __syncthreads();
+    // no barrier here: the next step reads only this thread's own svp/swp
+    // entries before its first block sum, and the reduction buffers of the
+    // two sums differ
   }
   if (i == n - 1) {
     cf x = __ldcg(A + (int64_t)(n - 1) * n + (n - 1));
@@ -586,6 +713,16 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     ee2[n - 1] = 0.0;
   }
   __syncthreads();
+  if constexpr (MODE == 1) {
+    double* side = S.side + ip * 6 * (int64_t)n;
+    for (int q = tid; q < n; q += kT) {
+      side[q] = dd[q];
+      side[n + q] = ee[q];
+    }
+    wy_factors(A, n, taur, taui, sY, tid, kT);
+    return;
+  }
+  }   // phase 1 (MODE != 2)
 
   // ---- 2. eigenvalues above β² (FP64 multisection) ----------------------------
   if (tid == 0) {
@@ -717,14 +854,15 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
     }
   }
   __syncthreads();
-  if (S.nuc) {   // nuclear norm of the patch (src/recon.jl:138-146): Σ σ_i = Σ √λ_i
+  if (MODE == 0 && S.nuc) {   // nuclear norm of the patch (src/recon.jl:138-146): Σ σ_i = Σ √λ_i
     const double sq = (tid < r) ? sqrt(fmax(lam[tid], 0.0)) : 0.0;
     const double tot = block_sum_d(sq, redd);
     if (tid == 0) S.nuc[ip] = tot;
     return;
   }
-  if (r == 0) {
-    for (int64_t q = tid; q < (int64_t)n * n; q += kT) Z[q] = make_float2(0.f, 0.f);
+  if (r == 0) {   // (the split stage's back-transform writes the zero columns itself)
+    if (MODE == 0)
+      for (int64_t q = tid; q < (int64_t)n * n; q += kT) Z[q] = make_float2(0.f, 0.f);
     return;
   }
 
@@ -820,6 +958,15 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
       }
       s0 = t;
     }
+  }
+  if constexpr (MODE == 2) {   // the eigenvalues and √-weights for the back-transform
+    double* side = S.side + ip * 6 * (int64_t)n;
+    float* sh = reinterpret_cast<float*>(side + 4 * (int64_t)n);
+    for (int q = tid; q < r; q += kT) {
+      side[3 * n + q] = lam[q];
+      sh[q] = hv[q];
+    }
+    return;
   }
 
   // ---- 4. V = H_0 ⋯ H_{n-2} Z, blocks of kNb reflectors from the last ---------
@@ -949,30 +1096,214 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
   }
 }
 
+// ---- split stage, third launch: Ṽ = conj(Q Z) diag(√h) -------------------------
+// One CTA per (32 eigenvectors, patch); warp w holds rows w, w + 16, … of its
+// 32 vectors in registers (lane = vector) through all WY blocks, taken from
+// the last reflector down: the block's Y (rows k0+1 … n−1, kYS-strided so a
+// row's 16 reflector entries load as warp-wide broadcasts) and T come into
+// shared memory; S = Yᴴ Z by per-warp partial sums added in warp order, S ←
+// T S, then Z −= Y S.  Columns at or beyond the patch's rank are written as
+// zeros.  FP32 throughout, as the one-launch stage's back-transform.
+constexpr int kYS = 18;        // row stride of the staged Y (16-byte aligned rows)
+constexpr int kWyThreads = 512;
+constexpr int kWyCols = 32;
+
+size_t wy_apply_smem(int nmax) {
+  return ((size_t)nmax * kYS + 16 * kNb * kWyCols + 2 * kNb * kWyCols + kNb * kNb) * sizeof(cf);
+}
+
+template <int RPW>
+__global__ void __launch_bounds__(kWyThreads, 1) k_wy_apply(EigArgs g) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  int s = 0;
+  while (s + 1 < g.nseg && (int64_t)blockIdx.y >= g.seg[s + 1].first) ++s;
+  const Seg& S = g.seg[s];
+  const int n = S.n;
+  const int64_t ip = (int64_t)blockIdx.y - S.first;
+  const int cb = blockIdx.x * kWyCols;
+  if (cb >= n) return;   // the grid covers the launch's largest n
+  const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+  const cf* A = S.gram + ip * (int64_t)n * n;
+  cf* Z = S.zv + ip * (int64_t)n * n;
+  const int r = S.rank[ip];
+  const int c = cb + lane;
+  if (cb >= r) {
+    if (c < n)
+      for (int row = w; row < n; row += kWyThreads / 32) Z[(int64_t)row * n + c] = make_float2(0.f, 0.f);
+    return;
+  }
+  const double* side = S.side + ip * 6 * (int64_t)n;
+  const float* hw = reinterpret_cast<const float*>(side + 4 * (int64_t)n);
+  cf* Ys = reinterpret_cast<cf*>(smraw);      // n × kYS
+  cf* part = Ys + (int64_t)n * kYS;           // 16 warps × kNb × 32
+  cf* Ss = part + 16 * kNb * kWyCols;         // kNb × 32
+  cf* S2 = Ss + kNb * kWyCols;                // kNb × 32
+  cf* Ts = S2 + kNb * kWyCols;                // kNb × kNb
+  float zr[RPW], zi[RPW];
+#pragma unroll
+  for (int q = 0; q < RPW; ++q) {
+    const int row = w + 16 * q;
+    zr[q] = (c < r && row < n) ? __ldcg(&Z[(int64_t)row * n + c].x) : 0.f;
+    zi[q] = 0.f;
+  }
+  const int nref = n - 1;
+  for (int kend = nref; kend > 0; kend -= kNb) {
+    const int k0 = max(0, kend - kNb);
+    const int nb = kend - k0;
+    const int blk = (nref - kend) / kNb;
+    const int m = n - k0 - 1;
+    for (int q = tid; q < m * kNb; q += kWyThreads) {   // row fastest: coalesced columns of A
+      const int jj = q / m, row = k0 + 1 + (q - jj * m);
+      const int k = k0 + jj;
+      cf y = make_float2(0.f, 0.f);
+      if (jj < nb) {
+        if (row == k + 1) y = make_float2(1.f, 0.f);
+        else if (row > k + 1) y = __ldcg(A + (int64_t)k * n + row);
+      }
+      Ys[row * kYS + jj] = y;
+    }
+    if (tid < kNb * kNb) Ts[tid] = __ldcg(A + upper_slot(n, blk * kNb * kNb + tid));
+    __syncthreads();
+    {   // partial S = Yᴴ Z over this warp's rows
+      float ar[kNb], ai[kNb];
+#pragma unroll
+      for (int a = 0; a < kNb; ++a) ar[a] = ai[a] = 0.f;
+#pragma unroll
+      for (int q = 0; q < RPW; ++q) {
+        const int row = w + 16 * q;
+        if (row > k0 && row < n) {
+          const float4* yr = reinterpret_cast<const float4*>(Ys + row * kYS);
+#pragma unroll
+          for (int h = 0; h < kNb / 2; ++h) {
+            const float4 y = yr[h];
+            ar[2 * h] += y.x * zr[q] + y.y * zi[q];
+            ai[2 * h] += y.x * zi[q] - y.y * zr[q];
+            ar[2 * h + 1] += y.z * zr[q] + y.w * zi[q];
+            ai[2 * h + 1] += y.z * zi[q] - y.w * zr[q];
+          }
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < kNb; ++a) part[(w * kNb + a) * kWyCols + lane] = make_float2(ar[a], ai[a]);
+    }
+    __syncthreads();
+    {
+      const int a = tid >> 5;   // kWyThreads / 32 = kNb rows of S
+      float sr = 0.f, si = 0.f;
+#pragma unroll
+      for (int w2 = 0; w2 < kWyThreads / 32; ++w2) {
+        const cf v = part[(w2 * kNb + a) * kWyCols + lane];
+        sr += v.x;
+        si += v.y;
+      }
+      Ss[a * kWyCols + lane] = make_float2(sr, si);
+    }
+    __syncthreads();
+    {
+      const int a = tid >> 5;
+      cf acc = make_float2(0.f, 0.f);
+      for (int b = a; b < kNb; ++b) acc = cadd(acc, cmul(Ts[a * kNb + b], Ss[b * kWyCols + lane]));
+      S2[a * kWyCols + lane] = acc;
+    }
+    __syncthreads();
+    {   // Z −= Y (T S) on this warp's rows
+      float sr[kNb], si[kNb];
+#pragma unroll
+      for (int a = 0; a < kNb; ++a) {
+        const cf v = S2[a * kWyCols + lane];
+        sr[a] = v.x;
+        si[a] = v.y;
+      }
+#pragma unroll
+      for (int q = 0; q < RPW; ++q) {
+        const int row = w + 16 * q;
+        if (row > k0 && row < n) {
+          const float4* yr = reinterpret_cast<const float4*>(Ys + row * kYS);
+          float tr = zr[q], ti = zi[q];
+#pragma unroll
+          for (int h = 0; h < kNb / 2; ++h) {
+            const float4 y = yr[h];
+            tr -= y.x * sr[2 * h] - y.y * si[2 * h];
+            ti -= y.x * si[2 * h] + y.y * sr[2 * h];
+            tr -= y.z * sr[2 * h + 1] - y.w * si[2 * h + 1];
+            ti -= y.z * si[2 * h + 1] + y.w * sr[2 * h + 1];
+          }
+          zr[q] = tr;
+          zi[q] = ti;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const float sh = (c < r) ? sqrtf(hw[c]) : 0.f;
+#pragma unroll
+  for (int q = 0; q < RPW; ++q) {
+    const int row = w + 16 * q;
+    if (row < n && c < n) Z[(int64_t)row * n + c] = make_float2(zr[q] * sh, -zi[q] * sh);
+  }
+}
+
 }  // namespace
 
 int eig2_prepare(int nmax) {
   if (nmax > kT) return fail(MSLR_ERR_UNSUPPORTED, "Gram side above 1024");
   if (smem_bytes(nmax, kT, 0) > smem_budget(kT))
     return fail(MSLR_ERR_UNSUPPORTED, "Gram side too large for the eigen stage");
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_budget(kT)));
-  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem_budget(kSmallT)));
+  const int big = (int)smem_budget(kT), small = (int)smem_budget(kSmallT);
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kT, 1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, small));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kT, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, small));
+  const int wy = (int)wy_apply_smem(kSmallT);
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_wy_apply<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, wy));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_wy_apply<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, wy));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_wy_apply<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, wy));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_wy_apply<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, wy));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_wy_apply<20>, cudaFuncAttributeMaxDynamicSharedMemorySize, wy));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_wy_apply<24>, cudaFuncAttributeMaxDynamicSharedMemorySize, wy));
   return MSLR_OK;
 }
 
 namespace {
 
-// One launch over segments that all take the same CTA variant.
+// The split stage applies to thresholded SVSTs (not the values-only or
+// all-eigenpairs modes) with a side buffer and 64 <= n <= 384 (the
+// back-transform's register tile; the T factors fit the upper triangle).
+// MSLR_EIG_SPLIT=0 keeps the one-launch stage everywhere (for comparisons).
+bool split_ok(const EigSegment& e) {
+  static const bool off = [] {
+    const char* v = std::getenv("MSLR_EIG_SPLIT");
+    return v && v[0] == '0';
+  }();
+  if (off || !e.side || e.nuc || e.lam_out || e.n < 64 || e.n > kSmallT) return false;
+  const int64_t nblk = (e.n - 1 + kNb - 1) / kNb;
+  return nblk * kNb * kNb <= (int64_t)e.n * (e.n - 1) / 2;
+}
+
+int wy_apply_launch(const EigArgs& a, int nmax, int64_t total, cudaStream_t st) {
+  const dim3 grid((unsigned)((nmax + kWyCols - 1) / kWyCols), (unsigned)total);
+  const size_t sm = wy_apply_smem(nmax);
+  const int rpw = (nmax + 15) / 16;
+  if (rpw <= 4) k_wy_apply<4><<<grid, kWyThreads, sm, st>>>(a);
+  else if (rpw <= 8) k_wy_apply<8><<<grid, kWyThreads, sm, st>>>(a);
+  else if (rpw <= 12) k_wy_apply<12><<<grid, kWyThreads, sm, st>>>(a);
+  else if (rpw <= 16) k_wy_apply<16><<<grid, kWyThreads, sm, st>>>(a);
+  else if (rpw <= 20) k_wy_apply<20><<<grid, kWyThreads, sm, st>>>(a);
+  else k_wy_apply<24><<<grid, kWyThreads, sm, st>>>(a);
+  return MSLR_OK;
+}
+
+// One launch (or, for the split stage, three) over segments that all take the
+// same CTA variant.
 int eig_launch_group(const std::vector<const EigSegment*>& segs, const double* thr, int thr_per_patch,
-                     cudaStream_t st) {
+                     cudaStream_t st, uint64_t* launches) {
   EigArgs a;
   a.nseg = (int)segs.size();
   a.thr = thr;
   a.thr_per_patch = thr_per_patch;
   int64_t total = 0;
   int nmax = 1;
+  bool split = true;
   for (int s = 0; s < a.nseg; ++s) {
     Seg& S = a.seg[s];
     const EigSegment& e = *segs[s];
@@ -986,19 +1317,36 @@ int eig_launch_group(const std::vector<const EigSegment*>& segs, const double* t
     S.lam = e.lam;
     S.nuc = e.nuc;
     S.lam_out = e.lam_out;
+    S.side = e.side;
     total += e.np;
     nmax = std::max(nmax, e.n);
+    split = split && split_ok(e);
   }
   bool big = nmax > kSmallT;
   for (const EigSegment* e : segs) big = big || e->big;
   const int threads = big ? kT : kSmallT;
+  if (split) {
+    a.rz = 0;
+    const size_t sm1 = vec_bytes(nmax) +
+                       std::max(threads <= kSmallT ? part_bytes(nmax) : (size_t)0, wy_bytes(nmax, threads)) + 128;
+    if (threads == kSmallT)
+      k_eig<kSmallT, 2, 1><<<(unsigned)total, kSmallT, sm1, st>>>(a);
+    else
+      k_eig<kT, 1, 1><<<(unsigned)total, kT, sm1, st>>>(a);
+    k_eig<kSmallT, kPairsMinB, 2><<<(unsigned)total, kSmallT, vec_bytes(nmax) + 128, st>>>(a);
+    wy_apply_launch(a, nmax, total, st);
+    MSLR_CUDA_TRY(cudaGetLastError());
+    if (launches) *launches += 3;
+    return MSLR_OK;
+  }
   a.rz = stage_cols(nmax, threads);
   const size_t sm = smem_bytes(nmax, threads, a.rz);
   if (threads == kSmallT)
-    k_eig<kSmallT, 2><<<(unsigned)total, kSmallT, sm, st>>>(a);
+    k_eig<kSmallT, 2, 0><<<(unsigned)total, kSmallT, sm, st>>>(a);
   else
-    k_eig<kT, 1><<<(unsigned)total, kT, sm, st>>>(a);
+    k_eig<kT, 1, 0><<<(unsigned)total, kT, sm, st>>>(a);
   MSLR_CUDA_TRY(cudaGetLastError());
+  if (launches) *launches += 1;
   return MSLR_OK;
 }
 
@@ -1009,21 +1357,22 @@ int eig_launch_group(const std::vector<const EigSegment*>& segs, const double* t
 // Per-patch thresholds (thr_per_patch) index patches across all segments, so
 // such calls keep every segment in one launch.
 int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int thr_per_patch,
-                     cudaStream_t st) {
+                     cudaStream_t st, uint64_t* launches) {
   if (nseg < 1 || nseg > kMaxSeg) return fail(MSLR_ERR_UNSUPPORTED, "too many scales in one launch");
   std::vector<const EigSegment*> small, big, all;
   for (int s = 0; s < nseg; ++s) {
     (segs[s].n <= kSmallT && !segs[s].big ? small : big).push_back(&segs[s]);
     all.push_back(&segs[s]);
   }
-  if (thr_per_patch || small.empty() || big.empty()) return eig_launch_group(all, thr, thr_per_patch, st);
-  int rc = eig_launch_group(big, thr, 0, st);
-  if (!rc) rc = eig_launch_group(small, thr, 0, st);
+  if (thr_per_patch || small.empty() || big.empty())
+    return eig_launch_group(all, thr, thr_per_patch, st, launches);
+  int rc = eig_launch_group(big, thr, 0, st, launches);
+  if (!rc) rc = eig_launch_group(small, thr, 0, st, launches);
   return rc;
 }
 
 int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, const double* thr,
-                int thr_per_patch, double lam, cudaStream_t st, int big) {
+                int thr_per_patch, double lam, cudaStream_t st, int big, double* side, uint64_t* launches) {
   EigSegment s;
   s.n = n;
   s.np = np;
@@ -1034,7 +1383,8 @@ int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, cons
   s.lam = lam;
   s.big = big;
   s.nuc = nullptr;
-  return eig_launch_multi(1, &s, thr, thr_per_patch, st);
+  s.side = side;
+  return eig_launch_multi(1, &s, thr, thr_per_patch, st, launches);
 }
 
 }  // namespace mslr

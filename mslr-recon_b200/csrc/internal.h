@@ -32,7 +32,7 @@ struct SvstWork {
   cf* gram = nullptr;        // np * n * n   Gram, then Householder vectors, then W
   cf* zv = nullptr;          // np * n * n   FP64 tridiagonal eigenvectors, then V (complex64)
   double* aux = nullptr;     // np * n * n   FP64 scratch for the twisted factorisations
-  double* vecs = nullptr;    // np * 6 * n   d, e, tau(re,im), eigenvalues, h
+  double* vecs = nullptr;    // np * 6 * n   split eigen stage: d, e of T, eigenvalues, √-weights h
   int* rank = nullptr;       // np          number of singular values above β
   cf* split_part = nullptr;  // nsplit * n * n partial Grams (split-K)
   int nsplit = 1;
@@ -231,12 +231,16 @@ struct EigSegment {
   double* nuc = nullptr;   // when set: per-patch Σ √λ above the threshold only (no vectors, no W)
   double* lam_out = nullptr;   // when set: every eigenpair — V (row-major, G = V Λ Vᴴ) in zv
                                // and the eigenvalues (descending, np × n) here; threshold unused
+  double* side = nullptr;      // np × 6n FP64 scratch; when set (and 64 <= n <= 384), the stage
+                               // runs as three launches (tridiagonalise, eigenpairs of T, V = Q Z)
 };
+// Adds the number of kernels launched to *launches when given.
 int eig_launch_multi(int nseg, const EigSegment* segs, const double* thr, int thr_per_patch,
-                     cudaStream_t st);
+                     cudaStream_t st, uint64_t* launches = nullptr);
 int eig2_prepare(int nmax);
 int eig2_launch(int n, int64_t np, cf* gram, cf* zv, float* aux, int* rank, const double* thr,
-                int thr_per_patch, double lam, cudaStream_t st, int big = 0);
+                int thr_per_patch, double lam, cudaStream_t st, int big = 0, double* side = nullptr,
+                uint64_t* launches = nullptr);
 
 // ---- cost evaluation (svst.cu, cost.cu) ------------------------------------------
 int patch_nucnorm_all(Ctx* c, const cf* X, double* reg_out, cudaStream_t st);

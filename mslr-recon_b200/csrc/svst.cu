@@ -366,9 +366,8 @@ int svst_core(const cf* in, const PatchMap& m, int64_t np, const WorkPtrs& w, in
               const DevWait& dw, cudaStream_t st, uint64_t* launches, int eig_big = 0) {
   int rc = svst_gram(in, m, np, w, nsplit, tc, dw, st, launches);
   if (rc) return rc;
-  if (launches) *launches += 1;
   rc = eig2_launch(m.n, np, w.gram, reinterpret_cast<cf*>(w.zv), reinterpret_cast<float*>(w.aux),
-                   w.rank, thr, thr_per_patch, lam, st, eig_big);
+                   w.rank, thr, thr_per_patch, lam, st, eig_big, w.vecs, launches);
   if (rc) return rc;
   if ((rc = svst_form_w(w, m.n, np, tc, dw, st, launches))) return rc;
   return svst_rebuild(in, m, np, w, out, direct, tc, dw, st, launches);
@@ -631,10 +630,9 @@ int patch_svst_from_gram(Ctx* c, int s, double beta, const cf* gram, const cf* i
   if ((rc = set_scalar(c->d_thr + 1, beta, st))) return rc;
   MSLR_CUDA_TRY(cudaMemcpyAsync(w.gram, gram, (size_t)g.n * g.n * sizeof(cf), cudaMemcpyDeviceToDevice, st));
   if ((rc = eig2_launch(g.n, 1, w.gram, reinterpret_cast<cf*>(w.zv), reinterpret_cast<float*>(w.aux), w.rank,
-                        c->d_thr + 1, 0, 1.0, st)))
+                        c->d_thr + 1, 0, 1.0, st, 0, w.vecs, &c->launches)))
     return rc;
   if ((rc = svst_form_w(w, g.n, 1, tc, ctx_wait(c), st, &c->launches))) return rc;
-  c->launches += 1;
   cf* dst = g.partition ? img_out : c->d_pbuf;
   if (g.partition && img_in == img_out) dst = c->d_img_tmp;
   if ((rc = svst_rebuild(img_in, m, 1, w, dst, g.partition ? 1 : 0, tc, ctx_wait(c), st, &c->launches)))
@@ -727,13 +725,9 @@ int patch_svst_all(Ctx* c, const double* thr_dev, const cf* Zin, cf* Xout, cudaS
     segs[k].rank = ws[k].rank;
     segs[k].lam = c->lambdas[k];
     segs[k].big = g.eig_big;
+    segs[k].side = ws[k].vecs;
   }
-  if ((rc = eig_launch_multi(c->Ns, segs.data(), thr_dev, 0, st))) return rc;
-  {
-    bool small = false, big = false;   // one eigen launch per CTA variant present
-    for (const auto& sg : segs) (sg.n <= 384 && !sg.big ? small : big) = true;
-    c->launches += (small && big) ? 2 : 1;
-  }
+  if ((rc = eig_launch_multi(c->Ns, segs.data(), thr_dev, 0, st, &c->launches))) return rc;
   for (int k = 0; k < c->Ns; ++k)
     if ((rc = svst_form_w(ws[k], c->scales[k].n, c->scales[k].Np, c->tc_mode(), ctx_wait(c), st,
                           &c->launches)))

@@ -80,7 +80,7 @@ NORMAL_TOL = {"plain": 1e-5, "tuned": 1e-5, "tuned-tc": 5e-5}   # FP32 FFTs; spl
 
 @pytest.mark.parametrize("form", ["plain", "tuned"])
 @pytest.mark.parametrize("m,n,batch", [(40, 12, 5), (12, 40, 5), (216, 64, 7), (64, 216, 3), (1000, 300, 2),
-                                       (1, 30, 4), (30, 1, 4)])
+                                       (1, 30, 4), (30, 1, 4), (150, 100, 3), (500, 384, 3), (63, 80, 3)])
 def test_svst_batch_vs_oracle(torch, M, m, n, batch, form):
     rng = np.random.default_rng(m * 1000 + n)
     X = (rng.standard_normal((batch, m, n)) + 1j * rng.standard_normal((batch, m, n))).astype(np.complex64)
