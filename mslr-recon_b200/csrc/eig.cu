@@ -186,6 +186,24 @@ int stage_cols(int n, int threads) {
   return rz;
 }
 
+__device__ __forceinline__ unsigned long long pk2(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long u) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(u));
+  return v;
+}
+// (a.x·b.x + c.x, a.y·b.y + c.y), each lane one correctly rounded FMA
+__device__ __forceinline__ unsigned long long fma2(unsigned long long a, unsigned long long b,
+                                                   unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
 // Eight columns of a tile row: the pending rank-2 update of element
 // (row, jb + b), its contribution to the row sum y_row and to the column
 // partials (cr, ci), written back.
@@ -237,9 +255,10 @@ __device__ __forceinline__ void col_sums(float* cr, float* ci, int lane) {
   ci[0] += __shfl_xor_sync(0xffffffffu, ci[0], 1);
 }
 
-// A tile (I, J), J < I, whose 32 rows and 32 columns all lie inside the
-// matrix: the same arithmetic as the general tile path without its
-// per-element tests; the column values come from the re-based vectors as
+// An off-diagonal tile (I, J), J < I, whose 32 columns all lie inside the
+// matrix (rows past n, in the last tile row, are masked per lane): the same
+// arithmetic as the general tile path without its per-element tests; the
+// column values come from the re-based vectors as
 // 16-byte loads, and each group's loads are issued before the previous
 // group is updated and stored (they address other columns) when PIPE (the
 // 384-thread variant; the 1024-thread variant's 64 registers do not hold
@@ -249,6 +268,7 @@ __device__ __noinline__ void full_tile(cf* A, int n, int o, int I, int J, int t,
                                        const cf* svr, const cf* svp, const cf* swp, const cf* sv, cf* part,
                                        cf* scol) {
   const int row = o + I * 32 + lane;
+  const bool rowok = row < n;   // the last tile row may reach past n (its vectors are zero there)
   const cf vpr = svp[row], wpr = swp[row], vr = sv[row];
   float yr = 0.f, yim = 0.f;
   const int jo = J * 32;   // first column − o
@@ -258,7 +278,7 @@ __device__ __noinline__ void full_tile(cf* A, int n, int o, int I, int J, int t,
   cf a[8];
   if constexpr (PIPE) {
 #pragma unroll
-    for (int b = 0; b < 8; ++b) a[b] = __ldcg(col0 + (int64_t)b * n);
+    for (int b = 0; b < 8; ++b) a[b] = rowok ? __ldcg(col0 + (int64_t)b * n) : make_float2(0.f, 0.f);
   }
 #pragma unroll 1
   for (int g8 = 0; g8 < 4; ++g8) {
@@ -266,17 +286,20 @@ __device__ __noinline__ void full_tile(cf* A, int n, int o, int I, int J, int t,
     if constexpr (PIPE) {
       if (g8 < 3) {
 #pragma unroll
-        for (int b = 0; b < 8; ++b) nx[b] = __ldcg(col0 + (int64_t)((g8 + 1) * 8 + b) * n);
+        for (int b = 0; b < 8; ++b)
+          nx[b] = rowok ? __ldcg(col0 + (int64_t)((g8 + 1) * 8 + b) * n) : make_float2(0.f, 0.f);
       }
     } else {
 #pragma unroll
-      for (int b = 0; b < 8; ++b) a[b] = __ldcg(col0 + (int64_t)(g8 * 8 + b) * n);
+      for (int b = 0; b < 8; ++b) a[b] = rowok ? __ldcg(col0 + (int64_t)(g8 * 8 + b) * n) : make_float2(0.f, 0.f);
     }
     float cr[8], ci[8];
     tile_group(a, pw + g8 * 8, vv + g8 * 4, vpr, wpr, vr, yr, yim, cr, ci);
     if (scol && g8 == 0) scol[row] = a[0];   // column o, the next step's
+    if (rowok) {
 #pragma unroll
-    for (int b = 0; b < 8; ++b) col0[(int64_t)(g8 * 8 + b) * n] = a[b];
+      for (int b = 0; b < 8; ++b) col0[(int64_t)(g8 * 8 + b) * n] = a[b];
+    }
     col_sums(cr, ci, lane);
     if ((lane & 3) == 0) part[(2 * t + 1) * 32 + g8 * 8 + (lane >> 2)] = make_float2(cr[0], ci[0]);
     if constexpr (PIPE) {
@@ -558,12 +581,22 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
       const int o = k + 1;
       const int T = (n - o + 31) >> 5;
       const int ntile = T * (T + 1) / 2;
-      for (int t = warp; t < ntile; t += nwarp) {
-        int I = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
-        while ((I + 1) * (I + 2) / 2 <= t) ++I;
-        while (I * (I + 1) / 2 > t) --I;
-        const int J = t - I * (I + 1) / 2;
-        if (I != J && o + I * 32 + 32 <= n) {
+      // work order: the T diagonal tiles (the costlier general path) first,
+      // one per warp, then the off-diagonal tiles row by row; t is the
+      // tile's slot in the partial sums (row-major over the triangle)
+      for (int u = warp; u < ntile; u += nwarp) {
+        int I, J;
+        if (u < T) {
+          I = J = u;
+        } else {
+          const int q = u - T;   // q-th tile strictly below the diagonal
+          I = (int)((1.f + sqrtf(8.f * (float)q + 1.f)) * 0.5f);
+          while (I > 1 && I * (I - 1) / 2 > q) --I;
+          while ((I + 1) * I / 2 <= q) ++I;
+          J = q - I * (I - 1) / 2;
+        }
+        const int t = I * (I + 1) / 2 + J;
+        if (I != J) {   // off-diagonal tiles: every column inside the matrix
           full_tile<(MAXT <= kSmallT)>(A, n, o, I, J, t, lane, spw, svr, svp, swp, sv, part,
                                        J == 0 ? scol : nullptr);
           continue;
@@ -1099,17 +1132,49 @@ __global__ void __launch_bounds__(MAXT, MINB) k_eig(EigArgs g) {
 // ---- split stage, third launch: Ṽ = conj(Q Z) diag(√h) -------------------------
 // One CTA per (32 eigenvectors, patch); warp w holds rows w, w + 16, … of its
 // 32 vectors in registers (lane = vector) through all WY blocks, taken from
-// the last reflector down: the block's Y (rows k0+1 … n−1, kYS-strided so a
-// row's 16 reflector entries load as warp-wide broadcasts) and T come into
-// shared memory; S = Yᴴ Z by per-warp partial sums added in warp order, S ←
-// T S, then Z −= Y S.  Columns at or beyond the patch's rank are written as
-// zeros.  FP32 throughout, as the one-launch stage's back-transform.
+// the last reflector down.  Each block's Y (rows k0+1 … n−1, kYS-strided so a
+// row's 16 reflector entries load as warp-wide broadcasts) and T arrive by
+// cp.async into one of two buffers while the previous block is applied:
+// S = Yᴴ Z by per-warp partial sums added in warp order, S ← T S, then
+// Z −= Y S.  The complex products run as packed FP32x2 FMAs on lane-wise
+// products, (y.re·z.re, y.im·z.im) and (y.re·z.im, y.im·z.re), combined once
+// per row or per reflector.  Columns at or beyond the patch's rank are
+// written as zeros.
 constexpr int kYS = 18;        // row stride of the staged Y (16-byte aligned rows)
 constexpr int kWyThreads = 512;
 constexpr int kWyCols = 32;
 
 size_t wy_apply_smem(int nmax) {
-  return ((size_t)nmax * kYS + 16 * kNb * kWyCols + 2 * kNb * kWyCols + kNb * kNb) * sizeof(cf);
+  return ((size_t)2 * nmax * kYS + 16 * kNb * kWyCols + 2 * kNb * kWyCols + 2 * kNb * kNb) * sizeof(cf);
+}
+
+__device__ __forceinline__ void cpa8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Y rows k0+1 … n−1 of reflectors k0 … k0+nb−1 (the unit entry and the zeros
+// above it written directly) and the block's T into (ys, ts); thread t owns
+// row k0+1+t (m <= n − 1 < kWyThreads).
+__device__ __forceinline__ void wy_stage(const cf* A, int n, int kend, cf* ys, cf* ts, int tid) {
+  const int k0 = max(0, kend - kNb), nb = kend - k0;
+  const int blk = (n - 1 - kend) / kNb;
+  const int m = n - k0 - 1;
+  if (tid < m) {
+    const int row = k0 + 1 + tid;
+    cf* dst = ys + row * kYS;
+#pragma unroll
+    for (int jj = 0; jj < kNb; ++jj) {
+      const int k = k0 + jj;
+      if (jj < nb && row > k + 1) cpa8(dst + jj, A + (int64_t)k * n + row);
+      else dst[jj] = make_float2((jj < nb && row == k + 1) ? 1.f : 0.f, 0.f);
+    }
+  }
+  if (tid < kNb * kNb) cpa8(ts + tid, A + upper_slot(n, blk * kNb * kNb + tid));
+  cpa_commit();
 }
 
 template <int RPW>
@@ -1134,11 +1199,12 @@ __global__ void __launch_bounds__(kWyThreads, 1) k_wy_apply(EigArgs g) {
   }
   const double* side = S.side + ip * 6 * (int64_t)n;
   const float* hw = reinterpret_cast<const float*>(side + 4 * (int64_t)n);
-  cf* Ys = reinterpret_cast<cf*>(smraw);      // n × kYS
-  cf* part = Ys + (int64_t)n * kYS;           // 16 warps × kNb × 32
+  cf* Ybuf = reinterpret_cast<cf*>(smraw);    // two buffers of n × kYS
+  const int ystride = n * kYS;
+  cf* part = Ybuf + 2 * ystride;              // 16 warps × kNb × 32
   cf* Ss = part + 16 * kNb * kWyCols;         // kNb × 32
   cf* S2 = Ss + kNb * kWyCols;                // kNb × 32
-  cf* Ts = S2 + kNb * kWyCols;                // kNb × kNb
+  cf* Tbuf = S2 + kNb * kWyCols;              // two buffers of kNb × kNb
   float zr[RPW], zi[RPW];
 #pragma unroll
   for (int q = 0; q < RPW; ++q) {
@@ -1147,44 +1213,44 @@ __global__ void __launch_bounds__(kWyThreads, 1) k_wy_apply(EigArgs g) {
     zi[q] = 0.f;
   }
   const int nref = n - 1;
-  for (int kend = nref; kend > 0; kend -= kNb) {
+  if (nref > 0) wy_stage(A, n, nref, Ybuf, Tbuf, tid);
+  cpa_wait_all();
+  __syncthreads();
+  int buf = 0;
+  for (int kend = nref; kend > 0; kend -= kNb, buf ^= 1) {
     const int k0 = max(0, kend - kNb);
-    const int nb = kend - k0;
-    const int blk = (nref - kend) / kNb;
-    const int m = n - k0 - 1;
-    for (int q = tid; q < m * kNb; q += kWyThreads) {   // row fastest: coalesced columns of A
-      const int jj = q / m, row = k0 + 1 + (q - jj * m);
-      const int k = k0 + jj;
-      cf y = make_float2(0.f, 0.f);
-      if (jj < nb) {
-        if (row == k + 1) y = make_float2(1.f, 0.f);
-        else if (row > k + 1) y = __ldcg(A + (int64_t)k * n + row);
-      }
-      Ys[row * kYS + jj] = y;
-    }
-    if (tid < kNb * kNb) Ts[tid] = __ldcg(A + upper_slot(n, blk * kNb * kNb + tid));
-    __syncthreads();
-    {   // partial S = Yᴴ Z over this warp's rows
-      float ar[kNb], ai[kNb];
+    const cf* Ys = Ybuf + buf * ystride;
+    const cf* Ts = Tbuf + buf * kNb * kNb;
+    if (kend - kNb > 0)   // the next block, into the other buffers
+      wy_stage(A, n, kend - kNb, Ybuf + (buf ^ 1) * ystride, Tbuf + (buf ^ 1) * kNb * kNb, tid);
+    // partial S = Yᴴ Z over this warp's rows, eight reflectors per pass
 #pragma unroll
-      for (int a = 0; a < kNb; ++a) ar[a] = ai[a] = 0.f;
+    for (int h = 0; h < 2; ++h) {
+      unsigned long long P[8], Q[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) P[a] = Q[a] = 0ull;
 #pragma unroll
       for (int q = 0; q < RPW; ++q) {
         const int row = w + 16 * q;
         if (row > k0 && row < n) {
-          const float4* yr = reinterpret_cast<const float4*>(Ys + row * kYS);
+          const unsigned long long z1 = pk2(zr[q], zi[q]), z2 = pk2(zi[q], zr[q]);
+          const float4* yr = reinterpret_cast<const float4*>(Ys + row * kYS) + 4 * h;
 #pragma unroll
-          for (int h = 0; h < kNb / 2; ++h) {
-            const float4 y = yr[h];
-            ar[2 * h] += y.x * zr[q] + y.y * zi[q];
-            ai[2 * h] += y.x * zi[q] - y.y * zr[q];
-            ar[2 * h + 1] += y.z * zr[q] + y.w * zi[q];
-            ai[2 * h + 1] += y.z * zi[q] - y.w * zr[q];
+          for (int t = 0; t < 4; ++t) {
+            const float4 y = yr[t];
+            const unsigned long long y0 = pk2(y.x, y.y), y1 = pk2(y.z, y.w);
+            P[2 * t] = fma2(y0, z1, P[2 * t]);
+            Q[2 * t] = fma2(y0, z2, Q[2 * t]);
+            P[2 * t + 1] = fma2(y1, z1, P[2 * t + 1]);
+            Q[2 * t + 1] = fma2(y1, z2, Q[2 * t + 1]);
           }
         }
       }
 #pragma unroll
-      for (int a = 0; a < kNb; ++a) part[(w * kNb + a) * kWyCols + lane] = make_float2(ar[a], ai[a]);
+      for (int a = 0; a < 8; ++a) {   // conj(y)·z = (Σ y.re z.re + y.im z.im, Σ y.re z.im − y.im z.re)
+        const float2 p = upk2(P[a]), qq = upk2(Q[a]);
+        part[(w * kNb + 8 * h + a) * kWyCols + lane] = make_float2(p.x + p.y, qq.x - qq.y);
+      }
     }
     __syncthreads();
     {
@@ -1206,33 +1272,38 @@ __global__ void __launch_bounds__(kWyThreads, 1) k_wy_apply(EigArgs g) {
       S2[a * kWyCols + lane] = acc;
     }
     __syncthreads();
-    {   // Z −= Y (T S) on this warp's rows
-      float sr[kNb], si[kNb];
+    // Z −= Y (T S) on this warp's rows, eight reflectors per pass
 #pragma unroll
-      for (int a = 0; a < kNb; ++a) {
-        const cf v = S2[a * kWyCols + lane];
-        sr[a] = v.x;
-        si[a] = v.y;
+    for (int h = 0; h < 2; ++h) {
+      unsigned long long sa[8], sb[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        const cf v = S2[(8 * h + a) * kWyCols + lane];
+        sa[a] = pk2(v.x, v.y);
+        sb[a] = pk2(v.y, v.x);
       }
 #pragma unroll
       for (int q = 0; q < RPW; ++q) {
         const int row = w + 16 * q;
         if (row > k0 && row < n) {
-          const float4* yr = reinterpret_cast<const float4*>(Ys + row * kYS);
-          float tr = zr[q], ti = zi[q];
+          const float4* yr = reinterpret_cast<const float4*>(Ys + row * kYS) + 4 * h;
+          unsigned long long U = 0ull, V = 0ull;
 #pragma unroll
-          for (int h = 0; h < kNb / 2; ++h) {
-            const float4 y = yr[h];
-            tr -= y.x * sr[2 * h] - y.y * si[2 * h];
-            ti -= y.x * si[2 * h] + y.y * sr[2 * h];
-            tr -= y.z * sr[2 * h + 1] - y.w * si[2 * h + 1];
-            ti -= y.z * si[2 * h + 1] + y.w * sr[2 * h + 1];
+          for (int t = 0; t < 4; ++t) {
+            const float4 y = yr[t];
+            const unsigned long long y0 = pk2(y.x, y.y), y1 = pk2(y.z, y.w);
+            U = fma2(y0, sa[2 * t], U);
+            V = fma2(y0, sb[2 * t], V);
+            U = fma2(y1, sa[2 * t + 1], U);
+            V = fma2(y1, sb[2 * t + 1], V);
           }
-          zr[q] = tr;
-          zi[q] = ti;
+          const float2 u = upk2(U), v = upk2(V);   // y·s = (Σ y.re s.re − y.im s.im, Σ y.re s.im + y.im s.re)
+          zr[q] -= u.x - u.y;
+          zi[q] -= v.x + v.y;
         }
       }
     }
+    cpa_wait_all();
     __syncthreads();
   }
   const float sh = (c < r) ? sqrtf(hw[c]) : 0.f;
@@ -1254,6 +1325,8 @@ int eig2_prepare(int nmax) {
   MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, small));
   MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kT, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, small));
+  MSLR_CUDA_TRY(cudaFuncSetAttribute(k_eig<kSmallT, kPairsMinB, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(228 * 1024 / kPairsMinB - 1024)));
   const int wy = (int)wy_apply_smem(kSmallT);
   MSLR_CUDA_TRY(cudaFuncSetAttribute(k_wy_apply<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, wy));
   MSLR_CUDA_TRY(cudaFuncSetAttribute(k_wy_apply<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, wy));
