@@ -129,6 +129,26 @@ def test_svst_batch_full_scale(torch, M, form):
         assert rel(out[b], ref) < SVST_TOL[form], (b, rel(out[b], ref))
 
 
+@pytest.mark.parametrize("form", ["plain", "tuned"])
+def test_svst_batch_full_rank(torch, M, form):
+    """Every singular value above the threshold, as in the metric workload's
+    POGM iterates: 48 patches of 1000 × 300 (Gram side 300) with a small β,
+    so that all 300 eigenvectors of every patch are back-transformed; three
+    patches against the FP64 oracle."""
+    m, n, batch = 1000, 300, 48
+    rng = np.random.default_rng(300)
+    X = (rng.standard_normal((batch, m, n)) + 1j * rng.standard_normal((batch, m, n))).astype(np.complex64)
+    betas = [2.0 + 0.1 * (b % 5) for b in range(batch)]
+    assert min(np.linalg.svd(X[0], compute_uv=False)) > max(betas)
+    cm = np.ascontiguousarray(np.transpose(X, (0, 2, 1)))
+    from mslr_recon_b200.context import FORMS
+    out = M.svst_batch(dev(torch, cm), m, n, betas, form=FORMS[form]).cpu().numpy()
+    out = np.transpose(out, (0, 2, 1))
+    for b in (0, batch // 2, batch - 1):
+        ref = O.svst(X[b].astype(np.complex128), betas[b])
+        assert rel(out[b], ref) < SVST_TOL[form], (b, rel(out[b], ref))
+
+
 def test_svst_single_matrix(torch, M):
     rng = np.random.default_rng(12)
     X = (rng.standard_normal((50, 20)) + 1j * rng.standard_normal((50, 20))).astype(np.complex64)
