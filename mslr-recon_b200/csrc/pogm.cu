@@ -85,7 +85,45 @@ __global__ void __launch_bounds__(kRedThreads)
   const bool vec = (E % 2 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15u) == 0);
   const int64_t E2 = vec ? E / 2 : 0;
   const float4* G4 = reinterpret_cast<const float4*>(G);
-  for (int64_t e2 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e2 < E2;
+  if (ns == 2) {   // two scales: every load of a pair issued before its stores
+    const float4* X4 = reinterpret_cast<const float4*>(X);
+    float4* U4 = reinterpret_cast<float4*>(U);
+    float4* Z4 = reinterpret_cast<float4*>(Z);
+    float4* GO4 = reinterpret_cast<float4*>(Gold);
+    for (int64_t e2 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e2 < E2;
+         e2 += (int64_t)gridDim.x * blockDim.x) {
+      const int64_t o1 = E2 + e2;
+      const float4 g4 = G4[e2];
+      const float4 xa = X4[e2], ua = U4[e2], xb = X4[o1], ub = U4[o1];
+      const float4 go = sigtest ? GO4[e2] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const cf g0 = make_float2(g4.x, g4.y), g1 = make_float2(g4.z, g4.w);
+      r_g2 += (double)g0.x * g0.x + (double)g0.y * g0.y;
+      r_g2 += (double)g1.x * g1.x + (double)g1.y * g1.y;
+      if (sigtest) {
+        r_sig += (double)g0.x * go.x - (double)g0.y * go.y;
+        r_sig += (double)g1.x * go.z - (double)g1.y * go.w;
+        GO4[e2] = g4;
+      }
+      cf un0, un1, zn0, zn1;
+      {
+        const cf x0 = make_float2(xa.x, xa.y), x1 = make_float2(xa.z, xa.w);
+        const cf u0 = make_float2(ua.x, ua.y), u1 = make_float2(ua.z, ua.w);
+        one(g0, &x0, &u0, &un0, &zn0);
+        one(g1, &x1, &u1, &un1, &zn1);
+        U4[e2] = make_float4(un0.x, un0.y, un1.x, un1.y);
+        Z4[e2] = make_float4(zn0.x, zn0.y, zn1.x, zn1.y);
+      }
+      {
+        const cf x0 = make_float2(xb.x, xb.y), x1 = make_float2(xb.z, xb.w);
+        const cf u0 = make_float2(ub.x, ub.y), u1 = make_float2(ub.z, ub.w);
+        one(g0, &x0, &u0, &un0, &zn0);
+        one(g1, &x1, &u1, &un1, &zn1);
+        U4[o1] = make_float4(un0.x, un0.y, un1.x, un1.y);
+        Z4[o1] = make_float4(zn0.x, zn0.y, zn1.x, zn1.y);
+      }
+    }
+  }
+  for (int64_t e2 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; ns != 2 && e2 < E2;
        e2 += (int64_t)gridDim.x * blockDim.x) {
     const float4 g4 = G4[e2];
     const cf g0 = make_float2(g4.x, g4.y), g1 = make_float2(g4.z, g4.w);
