@@ -760,6 +760,32 @@ __global__ void k_csum(const cf* __restrict__ T, int nf, int ch, int64_t nvox, c
     const float4* t4 = reinterpret_cast<const float4*>(T);
     float4* o4 = reinterpret_cast<float4*>(out) + (int64_t)t0 * h;
     const float4* a4 = reinterpret_cast<const float4*>(ahy) + (int64_t)t0 * h;
+    if (ch == 6) {   // the compiled coil group: the six coil loads and g / A'y issued together
+      for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < h; o += step) {
+#pragma unroll 2
+        for (int f = 0; f < nf; ++f) {
+          const float4* src = t4 + (int64_t)f * 6 * h + o;
+          const int64_t i = (int64_t)f * h + o;
+          float4 w[6];
+#pragma unroll
+          for (int c = 0; c < 6; ++c) w[c] = src[c * h];
+          const float4 g = mode ? o4[i] : subtract ? a4[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+          float4 sm = w[0];
+#pragma unroll
+          for (int c = 1; c < 6; ++c) {
+            sm.x += w[c].x;
+            sm.y += w[c].y;
+            sm.z += w[c].z;
+            sm.w += w[c].w;
+          }
+          float4 v = make_float4(sm.x * scale, sm.y * scale, sm.z * scale, sm.w * scale);
+          if (mode) v = make_float4(g.x + v.x, g.y + v.y, g.z + v.z, g.w + v.w);
+          else if (subtract) v = make_float4(v.x - g.x, v.y - g.y, v.z - g.z, v.w - g.w);
+          o4[i] = v;
+        }
+      }
+      return;
+    }
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += step) {
       const int64_t f = i / h, o = i - f * h;
       const float4* src = t4 + f * ch * h + o;
