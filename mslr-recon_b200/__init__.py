@@ -10,7 +10,7 @@ for tests and benchmarks; Julia callers use ``julia/MSLRB200.jl``.
 from ._lib import MSLRError, lib  # noqa: F401  (loads libmslr.so; raises if absent)
 from .context import MSLRContext, fp32_peak, ong_lustig_lambdas, sampling  # noqa: F401
 from .recon import SVST, img2patches, patch_geometry, patches2img, patchSVST, svst_batch  # noqa: F401
-from .reconstruct import run_recon, run_recon_kspace, sos_normalize  # noqa: F401
+from .reconstruct import run_recon, run_recon_files, run_recon_kspace, sos_normalize  # noqa: F401
 
 __all__ = ["MSLRContext", "MSLRError", "SVST", "img2patches", "patches2img", "patchSVST",
-           "patch_geometry", "svst_batch", "run_recon", "run_recon_kspace", "sos_normalize", "ong_lustig_lambdas", "sampling", "fp32_peak"]
+           "patch_geometry", "svst_batch", "run_recon", "run_recon_files", "run_recon_kspace", "sos_normalize", "ong_lustig_lambdas", "sampling", "fp32_peak"]

@@ -17,6 +17,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libmslr.so")
+IO_LIB = os.path.join(HERE, "libmslrio.so")
+IO_SRC = os.path.join(CSRC, "matio.cpp")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
@@ -84,6 +86,22 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
     return LIB
 
 
+def build_io(force: bool = False, verbose: bool = False) -> str:
+    """Compile the host-only MAT v7.3 / HDF5 library libmslrio.so (g++, zlib)."""
+    hdr = os.path.join(ROOT, "include", "mslr_io.h")
+    if force or _stale(IO_LIB, [IO_SRC, hdr]):
+        cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
+        cmd = [cxx, "-std=c++17", "-O3", "-fPIC", "-shared", "-Wall", "-I", os.path.join(ROOT, "include"),
+               IO_SRC, "-o", IO_LIB, "-lz", "-pthread"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"g++ failed for matio.cpp:\n{r.stdout}\n{r.stderr}")
+    return IO_LIB
+
+
 if __name__ == "__main__":
     p = build(force="--force" in sys.argv, verbose="--verbose" in sys.argv)
     print(p)
+    print(build_io(force="--force" in sys.argv, verbose="--verbose" in sys.argv))

@@ -1,0 +1,380 @@
+"""MAT v7.3 / HDF5 reader and writer (libmslrio.so), on the CPU.
+
+The reference reads its coil maps and k-space through MAT.jl / HDF5.jl and
+saves its results through MAT.jl (scripts/reconstruct.jl:88,95,242-260).
+Neither Julia nor libhdf5 is in this image, so the checks are:
+
+- the pin: a MATLAB-written v7.3 file from scipy's test data
+  (``testhdf5_7.4_GLNX86.mat``, ``testdouble`` = 0:pi/4:2*pi, written by
+  MATLAB's libhdf5) read bit-exactly by the library and by the independent
+  pure-Python reader ``oracle/h5_oracle.py``; the same variable from its
+  MATLAB v5 twin (read by scipy.io.loadmat) agrees;
+- every file the library writes is decoded identically by the oracle reader
+  (a second implementation of the format), bit-exact;
+- files in the newer HDF5 structures the writer does not produce
+  (superblock 2, object header 2, link messages, layout 4 with single-chunk,
+  implicit and fixed-array chunk indexes, filter pipeline 2 with shuffle,
+  attribute 3, compact layout) are assembled here byte by byte from the
+  format specification and read back bit-exactly;
+- damaged and foreign files fail with a status, never a crash.
+"""
+import os
+import zlib
+
+import numpy as np
+import pytest
+
+from oracle import h5_oracle as H
+
+matio = pytest.importorskip("mslr_recon_b200.matio")
+
+SCIPY_DATA = os.path.join(os.path.dirname(__import__("scipy").__file__), "io", "matlab", "tests", "data")
+MATLAB_V73 = os.path.join(SCIPY_DATA, "testhdf5_7.4_GLNX86.mat")
+MATLAB_V5 = os.path.join(SCIPY_DATA, "testdouble_7.4_GLNX86.mat")
+
+
+# ───────────────────────── the pin: a MATLAB-written file ─────────────────────────
+
+@pytest.mark.skipif(not os.path.exists(MATLAB_V73), reason="scipy test data not installed")
+def test_matlab_written_file_bit_exact():
+    want = np.arange(9) * (np.pi / 4)
+    with matio.H5File(MATLAB_V73) as f:
+        assert f.userblock == 512
+        assert f.names() == ["testdouble"]
+        inf = f.info("/testdouble")
+        assert inf.shape == (9, 1) and inf.mclass == "double" and inf.layout == 1
+        a = f.read_raw("/testdouble")
+    assert np.array_equal(a.ravel(), want)            # bit-exact: MATLAB stored 0:pi/4:2*pi
+    o = H.OracleFile(MATLAB_V73)
+    b, attrs = o.read("/testdouble")
+    assert np.array_equal(a, b) and attrs["MATLAB_class"] == "double"
+    text, ver, endian = H.matlab_header(MATLAB_V73)
+    assert text.startswith("MATLAB 7.0 MAT-file") and ver == b"\x00\x02" and endian == b"IM"
+    assert matio.matread(MATLAB_V73)["testdouble"].shape == (9, 1)
+
+
+@pytest.mark.skipif(not (os.path.exists(MATLAB_V73) and os.path.exists(MATLAB_V5)),
+                    reason="scipy test data not installed")
+def test_v73_and_v5_files_agree():
+    a = matio.matread(MATLAB_V73)["testdouble"]
+    b = matio.matread(MATLAB_V5)["testdouble"]
+    assert a.shape == b.shape and np.array_equal(a, b)
+
+
+# ───────────────────────── writer ↔ reader ↔ oracle ─────────────────────────
+
+def _variables(rng):
+    c = (rng.standard_normal((3, 5, 7, 9)) + 1j * rng.standard_normal((3, 5, 7, 9))).astype(np.complex64)
+    return {
+        "X": c,
+        "Xd": c.astype(np.complex128)[:, :2],
+        "f32": rng.standard_normal((11, 13)).astype(np.float32),
+        "f64": rng.standard_normal((4, 1, 6)),
+        "vec": rng.standard_normal(10),
+        "i8": rng.integers(-128, 127, (5, 3), dtype=np.int8),
+        "u16": rng.integers(0, 65535, (7,), dtype=np.uint16),
+        "i32": rng.integers(-2**31, 2**31 - 1, (2, 3, 4), dtype=np.int32),
+        "u32": rng.integers(0, 2**32 - 1, (6, 2), dtype=np.uint32),
+        "i64": rng.integers(-2**62, 2**62, (3, 3), dtype=np.int64),
+        "u64": rng.integers(0, 2**63, (2, 5), dtype=np.uint64),
+        "mask": rng.random((4, 6, 5)) > 0.5,
+        "scalar_f": 2.5,
+        "scalar_i": 7,
+        "flag": True,
+        "text": "run_recon ✓",
+        "cells": [np.arange(3, dtype=np.int64), np.arange(4.0), "ab"],
+        "empty": np.zeros((0, 3)),
+        "r6": rng.standard_normal((2, 3, 1, 2, 3, 2)).astype(np.float32),
+    }
+
+
+def _as_written(v):
+    """What matread returns for a value matwrite was given."""
+    if isinstance(v, np.ndarray) and v.ndim == 1:
+        return v.reshape(1, -1)
+    return v
+
+
+def _equal(a, b):
+    if isinstance(a, list):
+        return isinstance(b, list) and len(a) == len(b) and all(_equal(_as_written(x), y) for x, y in zip(a, b))
+    if isinstance(a, np.ndarray):
+        return isinstance(b, np.ndarray) and a.shape == b.shape and a.dtype == b.dtype and np.array_equal(a, b)
+    return type(a) is type(b) and a == b
+
+
+@pytest.mark.parametrize("compress,chunk", [(False, 0), (True, 4 << 20), (True, 64), (True, 24)])
+def test_round_trip_every_type(tmp_path, compress, chunk):
+    rng = np.random.default_rng(7)
+    d = _variables(rng)
+    p = str(tmp_path / "v.mat")
+    matio.matwrite(p, d, compress=compress, chunk_bytes=chunk or (4 << 20))
+    r = matio.matread(p)
+    assert set(r) == set(d)
+    for k, v in d.items():
+        assert _equal(_as_written(v), r[k]), k
+
+
+@pytest.mark.parametrize("chunk", [0, 96, 4 << 20])
+def test_oracle_reads_what_the_library_writes(tmp_path, chunk):
+    rng = np.random.default_rng(11)
+    d = {k: v for k, v in _variables(rng).items() if isinstance(v, np.ndarray) and v.size and v.dtype != np.bool_}
+    p = str(tmp_path / "o.mat")
+    matio.matwrite(p, d, compress=chunk > 0, chunk_bytes=chunk or (4 << 20))
+    o = H.OracleFile(p)
+    assert o.base_field == 512 and o.sb == 512
+    assert o.eof_field == os.path.getsize(p)
+    text, ver, endian = H.matlab_header(p)
+    assert text.startswith("MATLAB 7.3 MAT-file") and ver == b"\x00\x02" and endian == b"IM"
+    names = sorted(n for n, _ in o.members(o.root))
+    assert names == sorted(d)
+    with matio.H5File(p) as f:
+        for k, v in d.items():
+            a, attrs = o.read("/" + k)
+            assert np.array_equal(a, _as_written(v)), k
+            assert a.dtype == v.dtype
+            assert np.array_equal(f.read_raw("/" + k), a), k
+            assert attrs["MATLAB_class"] == f.info("/" + k).mclass
+
+
+def test_many_chunks_multilevel_btree(tmp_path):
+    # 5000 chunks of one row each: three B-tree levels with 64 entries per node
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal((5000, 3)).astype(np.float32)
+    p = str(tmp_path / "m.mat")
+    matio.matwrite(p, {"a": a}, compress=True, chunk_bytes=12)
+    with matio.H5File(p) as f:
+        inf = f.info("/a")
+        assert inf.layout == 2 and inf.chunk[0] == 1 and inf.n_filters == 1
+        for t in (1, 3, 8):
+            f.nthreads = t
+            assert np.array_equal(f.read_raw("/a"), a)
+    b, _ = H.OracleFile(p).read("/a")
+    assert np.array_equal(b, a)
+
+
+def test_edge_chunks_and_incompressible_chunks(tmp_path):
+    rng = np.random.default_rng(5)
+    noise = rng.integers(0, 256, (37, 29, 3), dtype=np.uint8)       # does not compress: stored raw
+    zeros = np.zeros((37, 29, 3), dtype=np.uint8)                   # compresses
+    p = str(tmp_path / "e.mat")
+    matio.matwrite(p, {"noise": noise, "zeros": zeros}, compress=True, chunk_bytes=1000)
+    o = H.OracleFile(p)
+    for k, v in (("noise", noise), ("zeros", zeros)):
+        a, _ = o.read("/" + k)
+        assert np.array_equal(a, v)
+        assert np.array_equal(matio.h5read(p, k), v)
+    assert os.path.getsize(p) < noise.nbytes + 64 * 1024
+
+
+def test_large_complex_array_threads(tmp_path):
+    rng = np.random.default_rng(9)
+    x = (rng.standard_normal((6, 4, 30, 40, 50)) + 1j * rng.standard_normal((6, 4, 30, 40, 50))).astype(np.complex64)
+    p = str(tmp_path / "k.mat")
+    matio.matwrite(p, {"ksp_epi_zf": x}, compress=True, nthreads=8, chunk_bytes=1 << 18)
+    for t in (1, 8):
+        assert np.array_equal(matio.h5read(p, "ksp_epi_zf", nthreads=t), x)
+
+
+# ───────────────────────── newer HDF5 structures, assembled here ─────────────────────────
+
+def _u(v, n):
+    return int(v).to_bytes(n, "little")
+
+
+def _dt_float(size):
+    if size == 4:
+        props = _u(0, 2) + _u(32, 2) + bytes([23, 8, 0, 23]) + _u(127, 4)
+    else:
+        props = _u(0, 2) + _u(64, 2) + bytes([52, 11, 0, 52]) + _u(1023, 4)
+    return bytes([0x11, 0x20, 31 if size == 4 else 63, 0]) + _u(size, 4) + props
+
+
+def _dt_complex3(size):
+    """Compound datatype version 3 (packed member names, minimal offsets)."""
+    fs = size // 2
+    body = b""
+    for i, nm in enumerate((b"r", b"i")):
+        body += nm + b"\0" + _u(i * fs, 1) + _dt_float(fs)
+    return bytes([0x36, 2, 0, 0]) + _u(size, 4) + body
+
+
+def _space2(dims):
+    return bytes([2, len(dims), 0, 1]) + b"".join(_u(d, 8) for d in dims)
+
+
+def _attr3(name, value: bytes):
+    dt = bytes([0x13, 0, 0, 0]) + _u(len(value), 4)
+    sp = bytes([2, 0, 0, 0])
+    nm = name.encode() + b"\0"
+    return bytes([3, 0]) + _u(len(nm), 2) + _u(len(dt), 2) + _u(len(sp), 2) + b"\0" + nm + dt + sp + value
+
+
+class _V2File:
+    """Superblock 2, version-2 object headers, link messages (checksums are
+    written as zeros: the library does not verify them)."""
+
+    def __init__(self):
+        self.buf = bytearray(48)
+
+    def alloc(self, data: bytes) -> int:
+        a = len(self.buf)
+        self.buf += data
+        while len(self.buf) % 8:
+            self.buf.append(0)
+        return a
+
+    @staticmethod
+    def ohdr(msgs):
+        body = b"".join(bytes([t]) + _u(len(d), 2) + b"\0" + d for t, d in msgs)
+        return b"OHDR" + bytes([2, 0x02]) + _u(len(body), 4) + body + b"\0" * 4
+
+    def finish(self, links):
+        lmsgs = [(0x06, bytes([1, 0, len(n)]) + n.encode() + _u(a, 8)) for n, a in links]
+        root = self.alloc(self.ohdr(lmsgs))
+        sb = b"\x89HDF\r\n\x1a\n" + bytes([2, 8, 8, 0]) + _u(0, 8) + _u(2**64 - 1, 8) + _u(len(self.buf), 8) + \
+            _u(root, 8) + b"\0" * 4
+        self.buf[:48] = sb
+        return bytes(self.buf)
+
+
+def _shuffle(raw: bytes, es: int) -> bytes:
+    a = np.frombuffer(raw, np.uint8).reshape(-1, es)
+    return a.T.tobytes()
+
+
+def _filters2(es, level=4):
+    # version 2: shuffle (id 2) then deflate (id 1); no names for ids < 256
+    return bytes([2, 2]) + _u(2, 2) + _u(0, 2) + _u(1, 2) + _u(es, 4) + _u(1, 2) + _u(0, 2) + _u(1, 2) + _u(level, 4)
+
+
+def _chunks_rowmajor(a, cd):
+    grid = [-(-n // c) for n, c in zip(a.shape, cd)]
+    for idx in np.ndindex(*grid):
+        sl = tuple(slice(i * c, min((i + 1) * c, n)) for i, c, n in zip(idx, cd, a.shape))
+        blk = np.zeros(cd, a.dtype)
+        blk[tuple(slice(0, s.stop - s.start) for s in sl)] = a[sl]
+        yield blk.tobytes()
+
+
+def _v4_layout(index_type, cd, es, addr, extra=b"", flags=0):
+    nd = len(cd) + 1
+    return bytes([4, 2, flags, nd, 4]) + b"".join(_u(c, 4) for c in cd) + _u(es, 4) + bytes([index_type]) + \
+        extra + _u(addr, 8)
+
+
+def test_newer_structures_bit_exact(tmp_path):
+    rng = np.random.default_rng(21)
+    f = _V2File()
+    links = []
+    cls_attr = (0x0C, _attr3("MATLAB_class", b"single"))
+
+    # fixed-array index, filtered (shuffle + deflate), edge chunks, complex compound v3
+    fa = (rng.standard_normal((7, 10)) + 1j * rng.standard_normal((7, 10))).astype(np.complex64)
+    cd = (3, 4)
+    entries = []
+    for raw in _chunks_rowmajor(fa, cd):
+        z = zlib.compress(_shuffle(raw, 8), 4)
+        entries.append((f.alloc(z), len(z)))
+    dblk_addr = len(f.buf)
+    fadb = b"FADB" + bytes([0, 1]) + _u(0, 8) + b"".join(_u(a, 8) + _u(n, 4) + _u(0, 4) for a, n in entries) + \
+        b"\0" * 4
+    dblk = f.alloc(fadb)
+    assert dblk == dblk_addr
+    fahd = b"FAHD" + bytes([0, 1, 16, 10]) + _u(len(entries), 8) + _u(dblk, 8) + b"\0" * 4
+    hdr = f.alloc(fahd)
+    fadb_fixed = bytearray(fadb)
+    fadb_fixed[6:14] = _u(hdr, 8)
+    f.buf[dblk:dblk + len(fadb)] = fadb_fixed
+    oh = f.alloc(f.ohdr([(0x01, _space2(fa.shape)), (0x03, _dt_complex3(8)),
+                         (0x08, _v4_layout(3, cd, 8, hdr, extra=bytes([10]))), (0x0B, _filters2(8)), cls_attr]))
+    links.append(("fixed", oh))
+
+    # implicit index, unfiltered
+    im = rng.standard_normal((5, 6)).astype(np.float32)
+    data = b"".join(_chunks_rowmajor(im, (2, 6)))
+    a = f.alloc(data)
+    oh = f.alloc(f.ohdr([(0x01, _space2(im.shape)), (0x03, _dt_float(4)), (0x08, _v4_layout(2, (2, 6), 4, a)),
+                         cls_attr]))
+    links.append(("implicit", oh))
+
+    # single-chunk index, filtered
+    sc = rng.standard_normal((4, 9))
+    z = zlib.compress(_shuffle(sc.tobytes(), 8), 6)
+    a = f.alloc(z)
+    oh = f.alloc(f.ohdr([(0x01, _space2(sc.shape)), (0x03, _dt_float(8)),
+                         (0x08, _v4_layout(1, sc.shape, 8, a, extra=_u(len(z), 8) + _u(0, 4), flags=2)),
+                         (0x0B, _filters2(8, 6)), (0x0C, _attr3("MATLAB_class", b"double"))]))
+    links.append(("single", oh))
+
+    # compact layout (version 3)
+    cp = np.arange(6, dtype=np.float64).reshape(2, 3)
+    oh = f.alloc(f.ohdr([(0x01, _space2(cp.shape)), (0x03, _dt_float(8)),
+                         (0x08, bytes([3, 0]) + _u(cp.nbytes, 2) + cp.tobytes())]))
+    links.append(("compact", oh))
+
+    p = tmp_path / "v2.h5"
+    p.write_bytes(f.finish(links))
+    with matio.H5File(str(p)) as h:
+        assert sorted(h.names()) == ["compact", "fixed", "implicit", "single"]
+        assert h.userblock == 0
+        assert np.array_equal(h.read_raw("/fixed"), fa) and h.info("/fixed").mclass == "single"
+        assert h.info("/fixed").chunk[0] == 3 and h.info("/fixed").n_filters == 2
+        assert np.array_equal(h.read_raw("/implicit"), im)
+        assert np.array_equal(h.read_raw("/single"), sc) and h.info("/single").mclass == "double"
+        assert np.array_equal(h.read_raw("/compact"), cp) and h.info("/compact").layout == 0
+
+
+# ───────────────────────── failures are statuses ─────────────────────────
+
+def test_errors_are_reported(tmp_path):
+    with pytest.raises(matio.MatIOError) as e:
+        matio.H5File(str(tmp_path / "missing.mat"))
+    assert e.value.code == matio.ERR_IO
+    junk = tmp_path / "junk.mat"
+    junk.write_bytes(b"MATLAB 5.0 MAT-file" + bytes(3000))
+    with pytest.raises(matio.MatIOError) as e:
+        matio.H5File(str(junk))
+    assert e.value.code == matio.ERR_FORMAT
+
+    p = str(tmp_path / "ok.mat")
+    x = np.arange(24, dtype=np.float32).reshape(4, 6)
+    matio.matwrite(p, {"x": x}, compress=True, chunk_bytes=32)
+    with pytest.raises(matio.MatIOError) as e:
+        matio.h5read(p, "nope")
+    assert e.value.code == matio.ERR_NOTFOUND
+    with matio.H5File(p) as f:
+        wrong = np.empty(5, np.float32)
+        rc = matio.lib.mslrio_read_at(f._h, f.lookup("/x"), wrong.ctypes.data, wrong.nbytes, 1)
+        assert rc == matio.ERR_ARG
+
+    # every truncation of a valid file fails cleanly (status, not a crash) or reads correctly
+    blob = open(p, "rb").read()
+    for cut in range(520, len(blob), max(1, (len(blob) - 520) // 60)):
+        t = tmp_path / "cut.mat"
+        t.write_bytes(blob[:cut])
+        try:
+            got = matio.h5read(str(t), "x")
+            assert np.array_equal(got, x)
+        except matio.MatIOError as err:
+            assert err.code in (matio.ERR_FORMAT, matio.ERR_NOTFOUND, matio.ERR_UNSUPPORTED)
+
+    with pytest.raises(matio.MatIOError):
+        matio.matwrite(str(tmp_path / "bad.mat"), {"s": {"a": 1}})
+    assert not os.path.exists(tmp_path / "bad.mat")          # a failed write leaves no partial file
+    with pytest.raises(matio.MatIOError):
+        with matio.MatWriter(str(tmp_path / "dup.mat")) as w:
+            w.write("a", 1.0)
+            w.write("a", 2.0)
+
+
+def test_c_abi_exports():
+    import ctypes
+    lib = ctypes.CDLL(matio._LIB_PATH)
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "mslr_io.h")).read()
+    import re
+    names = set(re.findall(r"\b(mslrio_[a-z_]+)\s*\(", hdr))
+    assert len(names) == 13
+    for n in names:
+        assert hasattr(lib, n), n
