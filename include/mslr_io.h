@@ -11,13 +11,15 @@
  * A MAT v7.3 file is an HDF5 file behind a 512-byte MATLAB header (the HDF5
  * "user block").  The reader handles what MATLAB and libhdf5 write for such
  * files: superblocks 0-3; object headers 1 and 2 with continuation blocks;
- * symbol-table groups and compact link messages; fixed-point, IEEE float,
+ * symbol-table groups, compact link messages and dense link storage (a
+ * fractal heap with a one- or two-level name index); fixed-point, IEEE float,
  * complex (a compound of two floats named real/imag, r/i or re/im), string
  * and object-reference datatypes; contiguous, compact and chunked layouts
  * (layout messages 1-4; chunk indexes: version-1 B-tree, single chunk,
  * implicit, fixed array); the deflate, shuffle and Fletcher-32 filters.
- * Not handled (reported as MSLRIO_ERR_UNSUPPORTED): dense link storage
- * (fractal heaps), extensible-array and version-2 B-tree chunk indexes,
+ * Not handled (reported as MSLRIO_ERR_UNSUPPORTED): fractal heaps with
+ * filters, huge objects or nested indirect blocks, deeper name indexes,
+ * extensible-array and version-2 B-tree chunk indexes,
  * big-endian data, variable-length types, external and virtual storage.
  *
  * The writer produces the structure MATLAB writes for `save -v7.3`:

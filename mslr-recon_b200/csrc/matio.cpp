@@ -471,6 +471,144 @@ struct mslrio_file {
         return false;
     }
 
+    // One link message body (header message 0x06, or an object of a group's
+    // fractal heap): hard links are kept, soft and external links skipped.
+    void link_body(Cur c, std::vector<std::pair<std::string, uint64_t>>& out) const {
+        if (c.u(1) != 1) fail(MSLRIO_ERR_FORMAT, "link message: unknown version");
+        int fl = int(c.u(1));
+        int ltype = (fl & 0x08) ? int(c.u(1)) : 0;
+        if (fl & 0x04) c.skip(8);
+        if (fl & 0x10) c.skip(1);
+        size_t nl = size_t(c.u(1 << (fl & 3)));
+        const uint8_t* nm = c.take(nl);
+        if (ltype != 0) return;
+        out.emplace_back(std::string(reinterpret_cast<const char*>(nm), nl), c.u(so));
+    }
+
+    // ── dense link storage: fractal heap + version-2 B-tree name index ──
+    static int log2u(uint64_t v) {
+        int r = -1;
+        while (v) {
+            v >>= 1;
+            ++r;
+        }
+        return r;
+    }
+    struct FHeap {
+        int id_len = 0, flags = 0, width = 0, max_heap_bits = 0, rows = 0, off_bytes = 0, len_bytes = 0;
+        uint64_t max_obj = 0, start = 0, max_direct = 0, root = UNDEF;
+    };
+    FHeap fheap(uint64_t addr) const {
+        FHeap h;
+        Cur c = at(addr);
+        c.need(5);
+        if (memcmp(c.p, "FRHP", 4) != 0) fail(MSLRIO_ERR_FORMAT, "bad fractal heap header");
+        c.skip(4);
+        if (c.u(1) != 0) fail(MSLRIO_ERR_FORMAT, "fractal heap: unknown version");
+        h.id_len = int(c.u(2));
+        int filt = int(c.u(2));
+        h.flags = int(c.u(1));
+        h.max_obj = c.u(4);
+        c.u(sl);                 // next huge object id
+        c.u(so);                 // huge-object B-tree
+        c.u(sl);                 // free space in managed blocks
+        c.u(so);                 // free-space manager
+        for (int i = 0; i < 8; ++i) c.u(sl);   // managed / allocated / iterator / counts and sizes
+        h.width = int(c.u(2));
+        h.start = c.u(sl);
+        h.max_direct = c.u(sl);
+        h.max_heap_bits = int(c.u(2));
+        c.u(2);                  // starting rows of the root indirect block
+        h.root = c.u(so);
+        h.rows = int(c.u(2));
+        if (filt) fail(MSLRIO_ERR_UNSUPPORTED, "filtered fractal heaps are not supported");
+        if (h.width <= 0 || h.start == 0 || h.max_direct < h.start || h.max_heap_bits <= 0 || h.max_heap_bits > 64)
+            fail(MSLRIO_ERR_FORMAT, "fractal heap: bad doubling table");
+        h.off_bytes = (h.max_heap_bits + 7) / 8;
+        h.len_bytes = std::min((log2u(h.max_direct) + 7) / 8, log2u(h.max_obj) / 8 + 1);
+        return h;
+    }
+    // Bytes of one managed or tiny heap object named by its heap ID.
+    Cur fh_object(const FHeap& h, const uint8_t* id) const {
+        int type = (id[0] >> 4) & 3;
+        if (type == 2) {
+            size_t n = size_t(id[0] & 0x0F) + 1;
+            if (1 + n > size_t(h.id_len)) fail(MSLRIO_ERR_FORMAT, "tiny heap object too long");
+            return Cur{id + 1, id + 1 + n};
+        }
+        if (type != 0) fail(MSLRIO_ERR_UNSUPPORTED, "huge fractal-heap objects are not supported");
+        if (1 + h.off_bytes + h.len_bytes > h.id_len) fail(MSLRIO_ERR_FORMAT, "heap ID too short");
+        uint64_t off = le(id + 1, h.off_bytes), n = le(id + 1 + h.off_bytes, h.len_bytes);
+        if (h.rows == 0) return at(h.root + off, n);
+        Cur ib = at(h.root);
+        ib.need(4);
+        if (memcmp(ib.p, "FHIB", 4) != 0) fail(MSLRIO_ERR_FORMAT, "bad fractal heap indirect block");
+        ib.skip(5 + size_t(so) + size_t(h.off_bytes));
+        int direct_rows = log2u(h.max_direct) - log2u(h.start) + 2;
+        uint64_t base = 0;
+        for (int r = 0; r < h.rows; ++r) {
+            uint64_t bs = r == 0 ? h.start : h.start << (r - 1);
+            for (int col = 0; col < h.width; ++col) {
+                uint64_t child = ib.u(so);
+                if (off >= base && off < base + bs) {
+                    if (r >= direct_rows)
+                        fail(MSLRIO_ERR_UNSUPPORTED, "nested fractal-heap indirect blocks are not supported");
+                    if (child == UNDEF || off - base + n > bs) fail(MSLRIO_ERR_FORMAT, "heap object outside its block");
+                    return at(child + (off - base), n);
+                }
+                base += bs;
+            }
+        }
+        fail(MSLRIO_ERR_FORMAT, "heap offset outside the heap");
+    }
+    void dense_links(uint64_t heap_addr, uint64_t bt2, std::vector<std::pair<std::string, uint64_t>>& out) const {
+        FHeap h = fheap(heap_addr);
+        Cur c = at(bt2);
+        c.need(4);
+        if (memcmp(c.p, "BTHD", 4) != 0) fail(MSLRIO_ERR_FORMAT, "bad v2 B-tree header");
+        c.skip(4);
+        if (c.u(1) != 0) fail(MSLRIO_ERR_FORMAT, "v2 B-tree: unknown version");
+        if (c.u(1) != 5) fail(MSLRIO_ERR_FORMAT, "link name index of the wrong type");
+        uint64_t node = c.u(4);
+        size_t rs = size_t(c.u(2));
+        int depth = int(c.u(2));
+        c.skip(2);
+        uint64_t root = c.u(so);
+        int nroot = int(c.u(2));
+        if (rs < 4 + size_t(h.id_len)) fail(MSLRIO_ERR_FORMAT, "v2 B-tree records too small");
+        if (depth > 1) fail(MSLRIO_ERR_UNSUPPORTED, "v2 B-tree name indexes deeper than one level");
+        auto records = [&](Cur& k, int n) {
+            for (int i = 0; i < n; ++i) {
+                const uint8_t* r = k.take(rs);
+                Cur obj = fh_object(h, r + 4);
+                link_body(obj, out);
+            }
+        };
+        if (root == UNDEF) return;
+        Cur k = at(root);
+        k.need(6);
+        if (depth == 0) {
+            if (memcmp(k.p, "BTLF", 4) != 0) fail(MSLRIO_ERR_FORMAT, "bad v2 B-tree leaf");
+            k.skip(6);
+            records(k, nroot);
+            return;
+        }
+        if (memcmp(k.p, "BTIN", 4) != 0) fail(MSLRIO_ERR_FORMAT, "bad v2 B-tree internal node");
+        k.skip(6);
+        records(k, nroot);
+        uint64_t leaf_max = (node - 10) / rs;
+        int nb = log2u(leaf_max) / 8 + 1;
+        for (int i = 0; i <= nroot; ++i) {
+            uint64_t child = k.u(so);
+            int n = int(k.u(nb));
+            Cur l = at(child);
+            l.need(6);
+            if (memcmp(l.p, "BTLF", 4) != 0) fail(MSLRIO_ERR_FORMAT, "bad v2 B-tree leaf");
+            l.skip(6);
+            records(l, n);
+        }
+    }
+
     std::vector<std::pair<std::string, uint64_t>> members(uint64_t addr) const {
         std::vector<std::pair<std::string, uint64_t>> out;
         auto msgs = header(addr);
@@ -481,22 +619,14 @@ struct mslrio_file {
                 uint64_t bt = c.u(so), heap = c.u(so);
                 group_btree(bt, heap, out, 0);
             } else if (m.type == 0x06) {
-                if (c.u(1) != 1) fail(MSLRIO_ERR_FORMAT, "link message: unknown version");
-                int fl = int(c.u(1));
-                int ltype = (fl & 0x08) ? int(c.u(1)) : 0;
-                if (fl & 0x04) c.skip(8);
-                if (fl & 0x10) c.skip(1);
-                size_t nl = size_t(c.u(1 << (fl & 3)));
-                const uint8_t* nm = c.take(nl);
-                if (ltype != 0) continue;   // soft and external links are not followed
-                out.emplace_back(std::string(reinterpret_cast<const char*>(nm), nl), c.u(so));
+                link_body(c, out);
             } else if (m.type == 0x02) {
                 c.skip(1);
                 int fl = int(c.u(1));
                 if (fl & 1) c.skip(8);
-                uint64_t fheap = c.u(so);
-                if (fheap != UNDEF)
-                    fail(MSLRIO_ERR_UNSUPPORTED, "dense link storage (a fractal-heap group) is not supported");
+                uint64_t fh = c.u(so);
+                uint64_t bt2 = c.u(so);
+                if (fh != UNDEF) dense_links(fh, bt2, out);
             }
         }
         return out;

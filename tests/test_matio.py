@@ -325,6 +325,101 @@ def test_newer_structures_bit_exact(tmp_path):
         assert np.array_equal(h.read_raw("/compact"), cp) and h.info("/compact").layout == 0
 
 
+def _link(name, addr):
+    return bytes([1, 0, len(name)]) + name.encode() + _u(addr, 8)
+
+
+def _dense_group(f, links, indirect: bool, two_level: bool):
+    """A new-style group whose links live in a fractal heap (width 4, blocks of
+    512 bytes up to 64 KiB, 32-bit heap offsets, 7-byte heap IDs) indexed by a
+    version-2 B-tree of link-name records; returns its object-header address."""
+    start, width, hdr_len = 512, 4, 4 + 1 + 8 + 4
+    objs = [_link(n, a) for n, a in links]
+    blocks = []                       # (heap offset of block, [(heap offset of object, bytes)])
+    if not indirect:
+        blocks.append((0, []))
+        off = hdr_len
+        for o in objs:
+            blocks[0][1].append((off, o))
+            off += len(o)
+        assert off <= start
+    else:
+        # two rows of four 512-byte direct blocks; objects spread over blocks 0, 3 and 6
+        per = -(-len(objs) // 3)
+        for j, b in enumerate((0, 3, 6)):
+            boff = b * start
+            off = boff + hdr_len
+            part = []
+            for o in objs[j * per:(j + 1) * per]:
+                part.append((off, o))
+                off += len(o)
+            assert off <= boff + start
+            blocks.append((boff, part))
+    heap_hdr_addr = len(f.buf)        # the header is written last; its address is fixed here
+    f.alloc(bytes(200))
+    block_addr = {}
+    for boff, part in blocks:
+        img = bytearray(start)
+        img[:hdr_len] = b"FHDB" + bytes([0]) + _u(heap_hdr_addr, 8) + _u(boff, 4)
+        for off, o in part:
+            img[off - boff:off - boff + len(o)] = o
+        block_addr[boff] = f.alloc(bytes(img))
+    if indirect:
+        entries = b"".join(_u(block_addr.get(i * start, 2**64 - 1), 8) for i in range(2 * width))
+        root = f.alloc(b"FHIB" + bytes([0]) + _u(heap_hdr_addr, 8) + _u(0, 4) + entries + b"\0" * 4)
+        rows = 2
+    else:
+        root, rows = block_addr[0], 0
+    frhp = (b"FRHP" + bytes([0]) + _u(7, 2) + _u(0, 2) + bytes([0]) + _u(4096, 4) + _u(0, 8) + _u(2**64 - 1, 8) +
+            _u(0, 8) + _u(2**64 - 1, 8) + b"".join(_u(0, 8) for _ in range(8)) + _u(width, 2) + _u(start, 8) +
+            _u(65536, 8) + _u(32, 2) + _u(0, 2) + _u(root, 8) + _u(rows, 2) + b"\0" * 4)
+    f.buf[heap_hdr_addr:heap_hdr_addr + len(frhp)] = frhp
+    recs = [_u(zlib.crc32(n.encode()), 4) + bytes([0]) + _u(off, 4) + _u(len(o), 2)
+            for (n, _), (off, o) in zip(links, [x for _, part in blocks for x in part])]
+    node = 512
+    if not two_level:
+        leaf = f.alloc(b"BTLF" + bytes([0, 5]) + b"".join(recs) + b"\0" * 4)
+        bt_root, nroot, depth = leaf, len(recs), 0
+    else:
+        # internal root with one record between two leaves
+        half = len(recs) // 2
+        l0 = f.alloc(b"BTLF" + bytes([0, 5]) + b"".join(recs[:half]) + b"\0" * 4)
+        l1 = f.alloc(b"BTLF" + bytes([0, 5]) + b"".join(recs[half + 1:]) + b"\0" * 4)
+        nb = ((node - 10) // 11).bit_length() - 1
+        nb = nb // 8 + 1
+        bt_root = f.alloc(b"BTIN" + bytes([0, 5]) + recs[half] + _u(l0, 8) + _u(half, nb) + _u(l1, 8) +
+                          _u(len(recs) - half - 1, nb) + b"\0" * 4)
+        nroot, depth = 1, 1
+    bthd = f.alloc(b"BTHD" + bytes([0, 5]) + _u(node, 4) + _u(11, 2) + _u(depth, 2) + bytes([100, 40]) +
+                   _u(bt_root, 8) + _u(nroot, 2) + _u(len(recs), 8) + b"\0" * 4)
+    linfo = bytes([0, 0]) + _u(heap_hdr_addr, 8) + _u(bthd, 8)
+    ginfo = bytes([0, 0])
+    return f.alloc(f.ohdr([(0x02, linfo), (0x0A, ginfo)]))
+
+
+@pytest.mark.parametrize("indirect,two_level", [(False, False), (True, False), (True, True)])
+def test_dense_link_storage(tmp_path, indirect, two_level):
+    rng = np.random.default_rng(31)
+    f = _V2File()
+    arrays, links = {}, []
+    for i in range(20 if not indirect else 45):
+        a = rng.standard_normal((3, i + 1))
+        addr = f.alloc(a.tobytes())
+        oh = f.alloc(f.ohdr([(0x01, _space2(a.shape)), (0x03, _dt_float(8)),
+                             (0x08, bytes([3, 1]) + _u(addr, 8) + _u(a.nbytes, 8))]))
+        arrays[f"var{i:02d}"] = a
+        links.append((f"var{i:02d}", oh))
+    g = _dense_group(f, links, indirect, two_level)
+    p = tmp_path / "dense.h5"
+    p.write_bytes(f.finish([("grp", g)]))
+    with matio.H5File(str(p)) as h:
+        assert h.names() == ["grp"]
+        assert sorted(h.names("/grp")) == sorted(arrays)
+        for k, v in arrays.items():
+            assert np.array_equal(h.read_raw(f"/grp/{k}"), v), k
+        assert h.info("/grp").dtype == matio.GROUP
+
+
 # ───────────────────────── failures are statuses ─────────────────────────
 
 def test_errors_are_reported(tmp_path):
