@@ -177,8 +177,8 @@ class H5File:
         a = self.read_raw(inf.addr)
         if cls == "cell":
             return [self.read_matlab(int(r)) for r in a.ravel()]
-        if cls == "char":
-            return "".join(chr(c) for c in a.T.ravel())
+        if cls == "char":       # MATLAB char: UTF-16 code units, column-major
+            return np.ascontiguousarray(a.T).astype("<u2").tobytes().decode("utf-16-le", errors="replace")
         if cls == "logical":
             a = a.astype(np.bool_)
         if a.size == 1 and a.ndim == 2:
@@ -258,10 +258,10 @@ class MatWriter:
         if isinstance(v, dict):
             raise MatIOError(ERR_UNSUPPORTED, "struct values are not supported by matwrite here")
         if isinstance(v, str):
-            codes = np.array([ord(c) for c in v], dtype=np.uint16).reshape(len(v), 1)
             if not v:
                 return self._put(name, np.array([0, 0], dtype=np.uint64), U64, "char", 2, 1)
-            return self._put(name, codes, U16, "char", 2)
+            codes = np.frombuffer(v.encode("utf-16-le"), dtype="<u2")
+            return self._put(name, codes.reshape(codes.size, 1), U16, "char", 2)
         if isinstance(v, (list, tuple)):
             refs = []
             for item in v:

@@ -81,7 +81,7 @@ def _variables(rng):
         "scalar_f": 2.5,
         "scalar_i": 7,
         "flag": True,
-        "text": "run_recon ✓",
+        "text": "run_recon ✓ 𝛌",
         "cells": [np.arange(3, dtype=np.int64), np.arange(4.0), "ab"],
         "empty": np.zeros((0, 3)),
         "r6": rng.standard_normal((2, 3, 1, 2, 3, 2)).astype(np.float32),
