@@ -1375,7 +1375,9 @@ struct mslrio_writer {
         if (mclass && *mclass) attr_string(msgs, "MATLAB_class", mclass);
         if (int_decode >= 0) attr_int(msgs, "MATLAB_int_decode", int_decode, 4, true);
         if (empty) attr_int(msgs, "MATLAB_empty", 1, 1, false);
-        uint64_t oh = object_header(msgs, 7);
+        const int nmsgs = 4 + (chunked ? 1 : 0) + ((mclass && *mclass) ? 1 : 0) + (int_decode >= 0 ? 1 : 0) +
+                          (empty ? 1 : 0);
+        uint64_t oh = object_header(msgs, nmsgs);
         group(gname).members.emplace_back(vname, oh);
         return oh;
     }

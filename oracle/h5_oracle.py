@@ -80,21 +80,27 @@ class OracleFile:
         a = self.abs(addr)
         if b[a] != 1:
             raise H5OracleError("object header version outside the oracle's subset")
+        nmsgs = _u(b, a + 2, 2)
         hsize = _u(b, a + 8, 4)
         blocks = [(a + 16, a + 16 + hsize)]
         out = []
+        seen = 0
         while blocks:
             lo, hi = blocks.pop(0)
             p = lo
             while p + 8 <= hi:
                 mtype, msize, mflags = _u(b, p, 2), _u(b, p + 2, 2), b[p + 4]
                 data = b[p + 8:p + 8 + msize]
+                seen += 1
                 if mtype == 0x10:
                     ca, cl = _u(data, 0, self.so), _u(data, self.so, self.sl)
                     blocks.append((self.abs(ca), self.abs(ca) + cl))
                 else:
                     out.append((mtype, mflags, data))
                 p += 8 + msize
+        # the prefix's message count covers every message, continuations included
+        if seen != nmsgs:
+            raise H5OracleError(f"object header declares {nmsgs} messages and holds {seen}")
         return out
 
     def members(self, addr: int):

@@ -137,6 +137,64 @@ def test_oracle_reads_what_the_library_writes(tmp_path, chunk):
             assert attrs["MATLAB_class"] == f.info("/" + k).mclass
 
 
+def test_writer_follows_libhdf5_layout_rules(tmp_path):
+    """The structures libhdf5 itself checks or sizes from the superblock:
+    message counts (the oracle checks every header it parses), full-size
+    symbol and B-tree nodes, names sorted and bracketed by the group
+    B-tree's keys, the heap's free-list sentinel, chunk keys in order with
+    the right-most key one chunk past the last, exact contiguous sizes."""
+    rng = np.random.default_rng(13)
+    a = rng.standard_normal((7, 9, 5)).astype(np.float32)
+    d = {"zeta": a, "alpha": np.arange(10.0), "cell": [np.arange(2), np.arange(3.0)], "mid": 3}
+    p = str(tmp_path / "rules.mat")
+    matio.matwrite(p, d, compress=True, chunk_bytes=5 * 4 * 2)     # chunks of (1, 2, 5): 7 x 5 = 35 of them
+    o = H.OracleFile(p)
+    b, so = o.b, o.so
+    assert o.internal_k == 16 and o.leaf_k >= 4
+
+    def u(x, n=8):
+        return int.from_bytes(b[x:x + n], "little")
+
+    for group in ("/", "/#refs#"):
+        msgs = o.messages(o.lookup(group))
+        stab = [m for t, _, m in msgs if t == 0x11][0]
+        bt, heap = int.from_bytes(stab[:8], "little"), int.from_bytes(stab[8:16], "little")
+        h = o.abs(heap)
+        assert b[h:h + 4] == b"HEAP" and u(h + 16) == 1                  # free list: none
+        dseg, dsize = o.abs(u(h + 24)), u(h + 8)
+        assert dsize % 8 == 0
+        n = o.abs(bt)
+        assert b[n:n + 4] == b"TREE" and b[n + 4] == 0 and b[n + 5] == 0 and u(n + 6, 2) == 1
+        assert n + 24 + 33 * 8 + 32 * 8 <= len(b)                         # full node of 2K = 32 children
+        k0, child, k1 = u(n + 24), u(n + 32), u(n + 40)
+        names = [nm for nm, _ in o.members(o.lookup(group))]
+        assert names == sorted(names, key=lambda x: x.encode())
+        name_at = lambda off: b[dseg + off:b.index(b"\0", dseg + off)].decode()
+        assert name_at(k0) == "" and name_at(k1) == names[-1]
+        sn = o.abs(child)
+        assert b[sn:sn + 4] == b"SNOD" and u(sn + 6, 2) == len(names)
+        assert sn + 8 + 2 * o.leaf_k * 40 <= len(b)                      # full node of 2·leaf K entries
+
+    msgs = dict((t, m) for t, _, m in o.messages(o.lookup("/zeta")))
+    lay = msgs[0x08]
+    assert lay[0] == 3 and lay[1] == 2 and lay[2] == 4
+    cd = [int.from_bytes(lay[11 + 4 * i:15 + 4 * i], "little") for i in range(4)]
+    assert cd == [1, 2, 5, 4]
+    n = o.abs(int.from_bytes(lay[3:11], "little"))
+    assert b[n + 4] == 1 and b[n + 5] == 0 and u(n + 6, 2) == 35       # 35 chunks fit one leaf
+    ks = 8 + 8 * 4
+    keys = [tuple(u(n + 24 + i * (ks + so) + 8 + 8 * j) for j in range(4)) for i in range(36)]
+    assert keys[:-1] == sorted(keys[:-1]) and len(set(keys[:-1])) == 35
+    assert keys[-1] == (keys[-2][0] + 1, keys[-2][1] + 2, keys[-2][2] + 5, 4)
+    assert n + 24 + 65 * ks + 64 * so <= len(b)                           # full node of 2K = 64 children
+
+    p2 = str(tmp_path / "contig.mat")
+    matio.matwrite(p2, {"alpha": np.arange(10.0)})
+    o2 = H.OracleFile(p2)
+    msgs = dict((t, m) for t, _, m in o2.messages(o2.lookup("/alpha")))
+    assert msgs[0x08][:2] == bytes([3, 1]) and int.from_bytes(msgs[0x08][10:18], "little") == 80
+
+
 def test_many_chunks_multilevel_btree(tmp_path):
     # 5000 chunks of one row each: three B-tree levels with 64 entries per node
     rng = np.random.default_rng(3)
