@@ -123,6 +123,18 @@ int64_t prod(const int64_t* d, int r) {
     return n;
 }
 
+// Bytes of an array of dims d (r of them) with es-byte elements, failing
+// rather than wrapping when the file's sizes are absurd.
+size_t array_bytes(const int64_t* d, int r, size_t es) {
+    unsigned __int128 n = es;
+    for (int i = 0; i < r; ++i) {
+        if (d[i] < 0) fail(MSLRIO_ERR_FORMAT, "negative dimension");
+        n *= uint64_t(d[i]);
+        if (n > (unsigned __int128)(uint64_t(1) << 62)) fail(MSLRIO_ERR_FORMAT, "dataset size overflows");
+    }
+    return size_t(n);
+}
+
 int dtype_size(int code) {
     switch (code) {
         case MSLRIO_I8: case MSLRIO_U8: return 1;
@@ -845,6 +857,8 @@ struct mslrio_file {
         h.skip(5);
         int client = int(h.u(1));
         int esz = int(h.u(1));
+        if (esz < so || (client == 1 && (esz - so - 4 < 1 || esz - so - 4 > 8)))
+            fail(MSLRIO_ERR_FORMAT, "fixed array: bad entry size");
         int pbits = int(h.u(1));
         uint64_t nmax = h.u(sl);
         uint64_t dblk = h.u(so);
@@ -922,7 +936,7 @@ struct mslrio_file {
         if (!ds.t.code) fail(MSLRIO_ERR_UNSUPPORTED, "datatype not supported: " + ds.t.why);
         size_t es = ds.t.size;
         int rank = ds.s.rank;
-        size_t n = ds.s.null ? 0 : size_t(prod(ds.s.dims, rank)) * es;
+        size_t n = ds.s.null ? 0 : array_bytes(ds.s.dims, rank, es);
         if (n != dst_bytes) fail(MSLRIO_ERR_ARG, "destination size does not match the dataset");
         if (n == 0) return;
         if (ds.layout == 0) {
@@ -947,7 +961,8 @@ struct mslrio_file {
             if (ds.cdims[d] <= 0) fail(MSLRIO_ERR_FORMAT, "zero chunk dimension");
             grid[d] = (ds.s.dims[d] + ds.cdims[d] - 1) / ds.cdims[d];
         }
-        size_t chunk_bytes = size_t(prod(ds.cdims, rank)) * es;
+        size_t chunk_bytes = array_bytes(ds.cdims, rank, es);
+        if (chunk_bytes >= (size_t(1) << 32)) fail(MSLRIO_ERR_FORMAT, "chunk of 4 GiB or more");
         int64_t ntot = prod(grid, rank);
         std::vector<ChunkRec> recs;
         if (ds.addr != UNDEF) {

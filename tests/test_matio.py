@@ -521,6 +521,54 @@ def test_errors_are_reported(tmp_path):
             w.write("a", 2.0)
 
 
+_FUZZ = r"""
+import os, resource, sys
+import numpy as np
+sys.path.insert(0, os.environ["REPO"])
+resource.setrlimit(resource.RLIMIT_AS, (6 << 30, 6 << 30))
+from mslr_recon_b200 import matio
+src, dst = sys.argv[1], sys.argv[2]
+blob = bytearray(open(src, "rb").read())
+rng = np.random.default_rng(int(sys.argv[3]))
+n_ok = n_err = 0
+for trial in range(150):
+    b = bytearray(blob)
+    for _ in range(int(rng.integers(1, 4))):
+        i = int(rng.integers(512, len(b)))
+        b[i] = int(rng.integers(0, 256))
+    open(dst, "wb").write(b)
+    try:
+        matio.matread(dst, nthreads=2)
+        n_ok += 1
+    except Exception:
+        n_err += 1
+print(n_ok, n_err)
+"""
+
+
+def test_damaged_files_never_crash(tmp_path):
+    """Random byte changes in a valid file (outside the MATLAB header) give a
+    result or an exception, never a crash; run in a child process whose
+    address space is capped, so that an absurd size read from the damage
+    fails as an allocation error instead of exhausting memory."""
+    import subprocess
+    import sys
+    rng = np.random.default_rng(17)
+    d = {"x": (rng.standard_normal((4, 6, 5)) + 1j * rng.standard_normal((4, 6, 5))).astype(np.complex64),
+         "c": [np.arange(3.0), "abc"], "m": rng.random((5, 5)) > 0.5, "s": 3.5}
+    src = str(tmp_path / "src.mat")
+    matio.matwrite(src, d, compress=True, chunk_bytes=64)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = tmp_path / "fuzz.py"
+    script.write_text(_FUZZ)
+    for seed in (1, 2):
+        r = subprocess.run([sys.executable, str(script), src, str(tmp_path / "dst.mat"), str(seed)],
+                           capture_output=True, text=True, timeout=300, env={**os.environ, "REPO": root})
+        assert r.returncode == 0, (r.returncode, r.stderr[-2000:])
+        ok, err = (int(v) for v in r.stdout.split())
+        assert ok + err == 150
+
+
 def test_c_abi_exports():
     import ctypes
     lib = ctypes.CDLL(matio._LIB_PATH)
