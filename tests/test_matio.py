@@ -61,6 +61,23 @@ def test_v73_and_v5_files_agree():
     assert a.shape == b.shape and np.array_equal(a, b)
 
 
+def test_v5_files_use_the_same_dims_convention(tmp_path):
+    """Coil maps saved by MATLAB without -v7.3 are MAT v5 files (read through
+    scipy.io.loadmat); they come back in the reversed-dims convention of the
+    v7.3 reader, so both kinds feed run_recon_files alike."""
+    from scipy.io import savemat
+    rng = np.random.default_rng(23)
+    sm = (rng.standard_normal((5, 4, 3, 2)) + 1j * rng.standard_normal((5, 4, 3, 2))).astype(np.complex64)
+    # a MATLAB array of size (Nx, Ny, Nz, Nc) = (5, 4, 3, 2), column-major
+    p5, p73 = str(tmp_path / "smaps_v5.mat"), str(tmp_path / "smaps_v73.mat")
+    savemat(p5, {"smaps": np.asfortranarray(sm), "R": 2.5})
+    matio.matwrite(p73, {"smaps": np.ascontiguousarray(sm.T), "R": 2.5})
+    a, b = matio.matread(p5), matio.matread(p73)
+    assert a["smaps"].shape == b["smaps"].shape == (2, 3, 4, 5)
+    assert np.array_equal(a["smaps"], b["smaps"]) and np.array_equal(a["smaps"], sm.T)
+    assert a["R"] == b["R"] == 2.5
+
+
 # ───────────────────────── writer ↔ reader ↔ oracle ─────────────────────────
 
 def _variables(rng):
