@@ -129,8 +129,11 @@ def run_recon_files(fn_ksp: str, fn_smaps: str, fn_recon_base: str, N, Nvc: int,
     cost logging) and saves ``fn_recon_base * "_<Ns>scales.mat"`` with the
     reference's sixteen variables (:242-260) through matwrite.  Array dims
     follow the reference's Julia arrays (so X is MATLAB (Nx,Ny,Nz,Nt,Ns)).
-    Returns the output path and the result dict."""
+    Returns the output path and the result dict (with ``seconds``: the wall
+    time of reading, reconstructing and writing)."""
+    import time
     from .matio import h5read, matread, matwrite
+    t0 = time.perf_counter()
     Nx, Ny, Nz = (int(v) for v in N)
     smaps_raw = np.asarray(matread(fn_smaps, nthreads)["smaps"])
     ksp = h5read(fn_ksp, "ksp_epi_zf", nthreads)
@@ -138,9 +141,11 @@ def run_recon_files(fn_ksp: str, fn_smaps: str, fn_recon_base: str, N, Nvc: int,
         raise ValueError(f"Unexpected k-space shape: {tuple(reversed(ksp.shape))}")
     if smaps_raw.shape != (Nvc, Nz, Ny, Nx):
         raise ValueError(f"Unexpected coil-map shape: {tuple(reversed(smaps_raw.shape))}")
+    t1 = time.perf_counter()
     out = run_recon_kspace(ksp.astype(np.complex64, copy=False), smaps_raw.astype(np.complex64, copy=False),
                            PATCH_SIZES, STRIDES, NITERS, sigma1=sigma1A_precomputed, form=form, log_costs=True)
     del ksp
+    t2 = time.perf_counter()
     # Ω (Nx, Ny, Nz, Nt) from the per-frame sample indices, R from frame 1 (:108-109)
     omega = np.zeros((Nt, Nz * Ny * Nx), dtype=np.bool_)
     omega[np.arange(Nt)[:, None], out["idx"].astype(np.int64)] = True
@@ -168,4 +173,5 @@ def run_recon_files(fn_ksp: str, fn_smaps: str, fn_recon_base: str, N, Nvc: int,
     }, compress=compress, nthreads=nthreads)
     out["omega"] = omega
     out["R"] = R
+    out["seconds"] = {"read": t1 - t0, "reconstruct": t2 - t1, "write": time.perf_counter() - t2}
     return fn_out, out
