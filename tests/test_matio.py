@@ -586,6 +586,61 @@ def test_damaged_files_never_crash(tmp_path):
         assert ok + err == 150
 
 
+_C_PROGRAM = r"""
+#include <stdio.h>
+#include <string.h>
+#include "mslr_io.h"
+int main(int argc, char** argv) {
+    float data[2 * 3 * 4 * 2];
+    for (int i = 0; i < 48; ++i) data[i] = (float)i - 7.5f;
+    int64_t dims[3] = {2, 3, 4};
+    mslrio_writer* w = NULL;
+    uint64_t a = 0;
+    if (mslrio_create(argv[1], 1, &w)) return 1;
+    if (mslrio_write(w, "ksp_epi_zf", MSLRIO_C64, 3, dims, data, "single", -1, 0, 6, 32, 2, &a)) return 2;
+    if (mslrio_finish(w)) return 3;
+    mslrio_file* f = NULL;
+    if (mslrio_open(argv[1], &f)) return 4;
+    uint64_t addr = 0;
+    mslrio_info info;
+    if (mslrio_lookup(f, "/ksp_epi_zf", &addr) || addr != a) return 5;
+    if (mslrio_info_at(f, addr, &info) || info.dtype != MSLRIO_C64 || info.rank != 3 || info.layout != 2) return 6;
+    if (strcmp(info.matlab_class, "single")) return 7;
+    float back[48];
+    if (mslrio_read_at(f, addr, back, sizeof(back), 0)) return 8;
+    if (memcmp(back, data, sizeof(back))) return 9;
+    if (mslrio_read_at(f, addr, back, 8, 1) != MSLRIO_ERR_ARG || !strlen(mslrio_last_error())) return 10;
+    if (mslrio_lookup(f, "/nope", &addr) != MSLRIO_ERR_NOTFOUND) return 11;
+    mslrio_close(f);
+    printf("ok\n");
+    return 0;
+}
+"""
+
+
+def test_c_header_from_c(tmp_path):
+    """include/mslr_io.h is plain C99 and the library works from a C program."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "t.c"
+    src.write_text(_C_PROGRAM)
+    exe = tmp_path / "t"
+    libdir = os.path.dirname(matio._LIB_PATH)
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(root, "include"), str(src), "-o",
+                        str(exe), "-L", libdir, "-l:libmslrio.so", "-Wl,-rpath," + libdir],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe), str(tmp_path / "c.mat")], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", (r.returncode, r.stdout, r.stderr)
+    b, _ = H.OracleFile(str(tmp_path / "c.mat")).read("/ksp_epi_zf")
+    want = (np.arange(48, dtype=np.float32) - 7.5).view(np.complex64).reshape(2, 3, 4)
+    assert np.array_equal(b, want)
+
+
 def test_c_abi_exports():
     import ctypes
     lib = ctypes.CDLL(matio._LIB_PATH)
